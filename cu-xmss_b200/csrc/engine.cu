@@ -1,0 +1,420 @@
+// Host engine of libxmss_b200 (see engine.h).
+#include "engine.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <tuple>
+
+#include "xmss_kernels.cuh"
+
+namespace xb {
+
+// Scratch budget of one chain launch when building trees: WOTS public keys
+// of at most this many bytes are live at once (2 GiB; HBM is 180 GB, this
+// keeps room for many concurrent tree node arrays).
+constexpr uint64_t kChainScratchBytes = 2ull << 30;
+
+DevBuf::~DevBuf()
+{
+    if (p_) cudaFree(p_);
+}
+
+void* DevBuf::get(size_t bytes)
+{
+    if (bytes == 0) bytes = 1;
+    if (bytes > cap_) {
+        size_t cap = std::max(bytes, cap_ + cap_ / 2);
+        cap = (cap + 4095) & ~(size_t)4095;
+        if (p_) {
+            XB_CUDA(cudaDeviceSynchronize());
+            XB_CUDA(cudaFree(p_));
+            p_ = nullptr;
+            cap_ = 0;
+        }
+        XB_CUDA(cudaMalloc(&p_, cap));
+        cap_ = cap;
+    }
+    return p_;
+}
+
+PinnedBuf::~PinnedBuf()
+{
+    if (p_) cudaFreeHost(p_);
+}
+
+void* PinnedBuf::get(size_t bytes)
+{
+    if (bytes == 0) bytes = 1;
+    if (bytes > cap_) {
+        size_t cap = std::max(bytes, cap_ + cap_ / 2);
+        cap = (cap + 4095) & ~(size_t)4095;
+        if (p_) {
+            XB_CUDA(cudaDeviceSynchronize());
+            XB_CUDA(cudaFreeHost(p_));
+            p_ = nullptr;
+            cap_ = 0;
+        }
+        XB_CUDA(cudaMallocHost(&p_, cap));
+        cap_ = cap;
+    }
+    return p_;
+}
+
+// ---------------------------------------------------------------------------
+
+const FamilyOps* family_ops(unsigned func, unsigned n)
+{
+    switch (func) {
+        case XMSS_SHA2:
+            if (n == 32) return &kOpsSha256N32;
+            if (n == 24) return &kOpsSha256N24;
+            if (n == 64) return &kOpsSha512N64;
+            return nullptr;
+        case XMSS_SHAKE128:
+            return n == 32 ? &kOpsShake128N32 : nullptr;
+        case XMSS_SHAKE256:
+            if (n == 24) return &kOpsShake256N24;
+            if (n == 32) return &kOpsShake256N32;
+            if (n == 64) return &kOpsShake256N64;
+            return nullptr;
+        default:
+            return nullptr;
+    }
+}
+
+const FamilyOps* ops_for(const xmss_params& p)
+{
+    const FamilyOps* o = family_ops(p.func, p.n);
+    if (!o || p.wots_w != 16) throw std::invalid_argument("parameter set has no GPU implementation");
+    return o;
+}
+
+Engine& Engine::get()
+{
+    static std::mutex m;
+    static Engine* e = nullptr;
+    std::lock_guard<std::mutex> g(m);
+    if (!e) {
+        int dev = 0;
+        const char* env = getenv("XMSS_B200_DEVICE");
+        if (env) {
+            dev = atoi(env);
+        } else if (cudaGetDevice(&dev) != cudaSuccess) {
+            dev = 0;
+        }
+        e = new Engine(dev);  // lives until exit
+    }
+    return *e;
+}
+
+Engine::Engine(int device) : device_(device)
+{
+    int n = 0;
+    XB_CUDA(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) throw CudaFailure("no CUDA device " + std::to_string(device));
+    XB_CUDA(cudaSetDevice(device));
+    XB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    XB_CUDA(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming));
+    work_ = s_work_.as<unsigned long long>(4);
+    XB_CUDA(cudaMemset(work_, 0, 4 * sizeof(unsigned long long)));
+}
+
+Engine::~Engine() = default;
+
+void Engine::begin(cudaStream_t st)
+{
+    XB_CUDA(cudaSetDevice(device_));
+    if (have_done_) XB_CUDA(cudaStreamWaitEvent(st, done_, 0));
+    if (profiling) {
+        XB_CUDA(cudaEventSynchronize(done_));
+        for (auto& m : marks_) {
+            free_events_.push_back(m.a);
+            free_events_.push_back(m.b);
+        }
+        marks_.clear();
+    }
+}
+
+cudaEvent_t Engine::event()
+{
+    if (!free_events_.empty()) {
+        cudaEvent_t e = free_events_.back();
+        free_events_.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    XB_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+void Engine::mark(int phase, bool start, cudaStream_t st)
+{
+    if (!profiling) return;
+    if (start) {
+        marks_.push_back(Mark{phase, event(), nullptr});
+        XB_CUDA(cudaEventRecord(marks_.back().a, st));
+    } else {
+        marks_.back().b = event();
+        XB_CUDA(cudaEventRecord(marks_.back().b, st));
+    }
+}
+
+void Engine::phase_ms(double out[kPhases])
+{
+    for (int i = 0; i < kPhases; i++) out[i] = 0;
+    XB_CUDA(cudaSetDevice(device_));
+    if (have_done_) XB_CUDA(cudaEventSynchronize(done_));
+    for (auto& m : marks_) {
+        if (!m.b) continue;
+        float ms = 0;
+        XB_CUDA(cudaEventElapsedTime(&ms, m.a, m.b));
+        out[m.phase] += ms;
+    }
+}
+
+void Engine::end(cudaStream_t st)
+{
+    XB_CUDA(cudaGetLastError());
+    XB_CUDA(cudaEventRecord(done_, st));
+    have_done_ = true;
+}
+
+// ---------------------------------------------------------------------------
+// Small byte-moving kernels (family independent).
+// ---------------------------------------------------------------------------
+
+// pk = root || PUB_SEED; sk = 0^ib || SK_SEED || SK_PRF || root || PUB_SEED
+// (xmss_core.c:134-161) from seeds (SK_SEED || SK_PRF || PUB_SEED) and roots.
+__global__ void k_keypair_finish(const uint8_t* __restrict__ seeds, const uint8_t* __restrict__ nodes,
+                                 uint64_t tree_bytes, uint64_t root_off, uint32_t n, uint32_t ib,
+                                 uint32_t sk_bytes, uint32_t count, uint8_t* __restrict__ pk, uint8_t* __restrict__ sk)
+{
+    const uint32_t k = blockIdx.x;
+    if (k >= count) return;
+    const uint8_t* seed = seeds + (uint64_t)k * 3 * n;
+    const uint8_t* root = nodes + (uint64_t)k * tree_bytes + root_off;
+    uint8_t* P = pk + (uint64_t)k * 2 * n;
+    uint8_t* S = sk + (uint64_t)k * sk_bytes;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        P[i] = root[i];
+        P[n + i] = seed[2 * n + i];
+        S[ib + i] = seed[i];
+        S[ib + n + i] = seed[n + i];
+        S[ib + 2 * n + i] = root[i];
+        S[ib + 3 * n + i] = seed[2 * n + i];
+    }
+    for (uint32_t i = threadIdx.x; i < ib; i += blockDim.x) S[i] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Pipelines.
+// ---------------------------------------------------------------------------
+
+static void run_ltree(const FamilyOps* ops, const LeafRef* refs, uint32_t nslots, uint8_t* wpk, uint8_t* wpk2,
+                      uint8_t* leaf_out, const void* ctx, const int* status, cudaStream_t st)
+{
+    int cnt = (int)ops->len, level = 0;
+    uint8_t *src = wpk, *dst = wpk2;
+    uint32_t sstr = ops->len, dstr = (ops->len + 1) / 2;
+    while (cnt > 1) {
+        ops->ltree_level(refs, nslots, level, cnt, src, sstr, dst, dstr, leaf_out, ctx, status, st);
+        cnt = (cnt + 1) / 2;
+        std::swap(src, dst);
+        std::swap(sstr, dstr);
+        level++;
+    }
+}
+
+void Engine::build_trees(const FamilyOps* ops, const TreeJob* d_jobs, uint32_t njobs, int h, uint8_t* d_nodes,
+                         const void* d_ctx, cudaStream_t st)
+{
+    const uint64_t total = (uint64_t)njobs << h;
+    const uint64_t per_slot = (uint64_t)ops->len * ops->n;
+    const uint64_t cap = std::max<uint64_t>(1, std::min<uint64_t>(total, kChainScratchBytes / per_slot));
+    uint8_t* wpk = s_wpk_.as<uint8_t>(cap * per_slot);
+    uint8_t* wpk2 = s_wpk2_.as<uint8_t>(cap * ((ops->len + 1) / 2) * ops->n);
+    LeafRef* refs = s_refs_.as<LeafRef>(cap);
+    for (uint64_t s0 = 0; s0 < total; s0 += cap) {
+        const uint64_t ns = std::min(cap, total - s0);
+        mark(kChains, true, st);
+        ops->keygen_chains(d_jobs, h, s0, ns, d_ctx, wpk, refs, st);
+        mark(kChains, false, st);
+        mark(kLtree, true, st);
+        run_ltree(ops, refs, (uint32_t)ns, wpk, wpk2, d_nodes, d_ctx, nullptr, st);
+        mark(kLtree, false, st);
+    }
+    mark(kTree, true, st);
+    for (int level = 0; level < h; level++) ops->tree_level(d_jobs, njobs, h, level, d_nodes, d_ctx, st);
+    mark(kTree, false, st);
+}
+
+void Engine::keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_seeds,
+                     uint8_t* d_pk, uint8_t* d_sk, cudaStream_t st)
+{
+    if (!count) return;
+    const uint32_t n = p.n, th = p.tree_height;
+    void* ctx = s_ctx_.get((size_t)count * ops->ctx_bytes);
+    ops->make_ctx(d_seeds + 2 * n, 3 * n, d_seeds, 3 * n, d_seeds + n, 3 * n, count, ctx, st);
+    const uint64_t tree_bytes = ((2ull << th) - 1) * n;
+    TreeJob* hj = h_jobs_.as<TreeJob>(count);
+    for (uint32_t k = 0; k < count; k++) hj[k] = TreeJob{k, p.d - 1, 0, (uint64_t)k * tree_bytes};
+    TreeJob* dj = s_jobs_.as<TreeJob>(count);
+    XB_CUDA(cudaMemcpyAsync(dj, hj, count * sizeof(TreeJob), cudaMemcpyHostToDevice, st));
+    uint8_t* nodes = s_nodes_.as<uint8_t>(count * tree_bytes);
+    build_trees(ops, dj, count, (int)th, nodes, ctx, st);
+    k_keypair_finish<<<count, 64, 0, st>>>(d_seeds, nodes, tree_bytes, level_offset((int)th, (int)th) * n, n,
+                                          p.index_bytes, (uint32_t)p.sk_bytes, count, d_pk, d_sk);
+    // the host job list is reused by the next call only after this one's
+    // copy has been consumed
+    XB_CUDA(cudaStreamSynchronize(st));
+}
+
+void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_sm,
+                    const uint64_t* d_sm_off, const uint64_t* d_smlen, const uint8_t* d_pk, uint32_t npk,
+                    const uint32_t* d_pk_index, int* d_status, cudaStream_t st)
+{
+    XB_CUDA(cudaMemsetAsync(work_, 0, 3 * sizeof(unsigned long long), st));
+    if (!count) return;
+    const uint32_t n = p.n, len = ops->len;
+    void* ctx = s_ctx_.get((size_t)npk * ops->ctx_bytes);
+    ops->make_ctx(d_pk + n, 2 * n, nullptr, 0, nullptr, 0, npk, ctx, st);
+    VerifyArgs v;
+    v.sm = d_sm;
+    v.sm_off = d_sm_off;
+    v.smlen = d_smlen;
+    v.key = d_pk_index;
+    v.key_root = d_pk;
+    v.key_stride = 2 * n;
+    v.node = s_node_.as<uint8_t>((size_t)count * n);
+    v.lens = s_lens_.as<uint8_t>((size_t)count * len);
+    v.idx = s_idx_.as<uint64_t>(count);
+    v.status = d_status;
+    v.wpk = s_wpk_.as<uint8_t>((size_t)count * len * n);
+    v.wpk2 = s_wpk2_.as<uint8_t>((size_t)count * ((len + 1) / 2) * n);
+    v.leaf = s_leaf_.as<uint8_t>((size_t)count * n);
+    v.refs = s_refs_.as<LeafRef>(count);
+    v.work = work_;
+    v.count = count;
+    v.index_bytes = p.index_bytes;
+    v.sig_bytes = p.sig_bytes;
+    v.tree_height = p.tree_height;
+    v.d = p.d;
+    mark(kPrep, true, st);
+    ops->verify_prep(v, ctx, st);
+    mark(kPrep, false, st);
+    for (uint32_t layer = 0; layer < p.d; layer++) {
+        mark(kChains, true, st);
+        ops->verify_chains(v, layer, ctx, st);
+        mark(kChains, false, st);
+        mark(kLtree, true, st);
+        run_ltree(ops, v.refs, count, v.wpk, v.wpk2, v.leaf, ctx, v.status, st);
+        mark(kLtree, false, st);
+        mark(kRoot, true, st);
+        ops->verify_root(v, layer, ctx, st);
+        mark(kRoot, false, st);
+    }
+}
+
+void Engine::last_verify_work(unsigned long long out[3])
+{
+    XB_CUDA(cudaSetDevice(device_));
+    if (have_done_) XB_CUDA(cudaEventSynchronize(done_));
+    XB_CUDA(cudaMemcpy(out, work_, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+}
+
+void Engine::sign(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* h_sk,
+                  const uint64_t* h_idx, uint8_t* d_sm, const uint64_t* d_sm_off, const uint64_t* d_mlen,
+                  cudaStream_t st)
+{
+    if (!count) return;
+    const uint32_t n = p.n, th = p.tree_height, d = p.d, ib = p.index_bytes;
+    const uint64_t skb = p.sk_bytes;
+    // Keys: distinct (SK_SEED, SK_PRF, root, PUB_SEED) tuples.
+    std::map<std::string, uint32_t> keyidx;
+    std::vector<uint32_t> req_key(count);
+    std::vector<uint8_t> keymat;  // nkeys x 4n
+    for (uint32_t r = 0; r < count; r++) {
+        std::string k((const char*)h_sk + r * skb + ib, 4 * n);
+        auto it = keyidx.find(k);
+        if (it == keyidx.end()) {
+            it = keyidx.emplace(k, (uint32_t)keyidx.size()).first;
+            keymat.insert(keymat.end(), k.begin(), k.end());
+        }
+        req_key[r] = it->second;
+    }
+    const uint32_t nkeys = (uint32_t)keyidx.size();
+    // Subtrees: distinct (key, layer, tree).
+    const uint64_t tree_bytes = ((2ull << th) - 1) * n;
+    std::map<std::tuple<uint32_t, uint32_t, uint64_t>, uint32_t> jobidx;
+    std::vector<TreeJob> jobs;
+    std::vector<uint64_t> tree_off((size_t)count * d);
+    for (uint32_t r = 0; r < count; r++) {
+        for (uint32_t l = 0; l < d; l++) {
+            const uint32_t sh = th * (l + 1);
+            const uint64_t tree = sh >= 64 ? 0 : (h_idx[r] >> sh);
+            auto key = std::make_tuple(req_key[r], l, tree);
+            auto it = jobidx.find(key);
+            if (it == jobidx.end()) {
+                it = jobidx.emplace(key, (uint32_t)jobs.size()).first;
+                jobs.push_back(TreeJob{req_key[r], l, tree, (uint64_t)jobs.size() * tree_bytes});
+            }
+            tree_off[(size_t)r * d + l] = jobs[it->second].node_off;
+        }
+    }
+    const uint32_t njobs = (uint32_t)jobs.size();
+    // Stage everything in one pinned block and one device block.
+    const size_t sz_keys = (size_t)nkeys * 4 * n, sz_jobs = njobs * sizeof(TreeJob),
+                 sz_toff = tree_off.size() * sizeof(uint64_t), sz_idx = count * sizeof(uint64_t),
+                 sz_key = count * sizeof(uint32_t);
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t o_jobs = al(sz_keys), o_toff = o_jobs + al(sz_jobs), o_idx = o_toff + al(sz_toff),
+                 o_key = o_idx + al(sz_idx), total = o_key + al(sz_key);
+    uint8_t* hs = h_jobs_.as<uint8_t>(total);
+    memcpy(hs, keymat.data(), sz_keys);
+    memcpy(hs + o_jobs, jobs.data(), sz_jobs);
+    memcpy(hs + o_toff, tree_off.data(), sz_toff);
+    memcpy(hs + o_idx, h_idx, sz_idx);
+    memcpy(hs + o_key, req_key.data(), sz_key);
+    uint8_t* ds = s_keys_.as<uint8_t>(total);
+    XB_CUDA(cudaMemcpyAsync(ds, hs, total, cudaMemcpyHostToDevice, st));
+    const uint8_t* dkeys = ds;
+    void* ctx = s_ctx_.get((size_t)nkeys * ops->ctx_bytes);
+    // key material rows: SK_SEED | SK_PRF | root | PUB_SEED
+    ops->make_ctx(dkeys + 3 * n, 4 * n, dkeys, 4 * n, dkeys + n, 4 * n, nkeys, ctx, st);
+    uint8_t* nodes = s_nodes_.as<uint8_t>(njobs * tree_bytes);
+    build_trees(ops, (const TreeJob*)(ds + o_jobs), njobs, (int)th, nodes, ctx, st);
+    SignArgs g;
+    g.sm = d_sm;
+    g.sm_off = d_sm_off;
+    g.mlen = d_mlen;
+    g.idx = (const uint64_t*)(ds + o_idx);
+    g.key = (const uint32_t*)(ds + o_key);
+    g.key_root = dkeys + 2 * n;
+    g.key_stride = 4 * n;
+    g.tree_off = (const uint64_t*)(ds + o_toff);
+    g.nodes = nodes;
+    g.lens = s_lens_.as<uint8_t>((size_t)count * d * ops->len);
+    g.count = count;
+    g.index_bytes = ib;
+    g.sig_bytes = p.sig_bytes;
+    g.tree_height = th;
+    g.d = d;
+    mark(kRoot, true, st);
+    ops->sign_prep(g, ctx, st);
+    mark(kRoot, false, st);
+    mark(kChains, true, st);
+    ops->sign_chains(g, ctx, st);
+    mark(kChains, false, st);
+    XB_CUDA(cudaStreamSynchronize(st));  // staging buffers are reused by the next call
+}
+
+void Engine::core_hash(const FamilyOps* ops, uint32_t count, const uint8_t* d_in, const uint64_t* d_off,
+                       const uint64_t* d_len, uint8_t* d_out, cudaStream_t st)
+{
+    ops->core_hash(d_in, d_off, d_len, count, d_out, st);
+}
+
+}  // namespace xb

@@ -1,0 +1,154 @@
+// Host engine of libxmss_b200: owns the CUDA stream, grow-only scratch
+// memory and the launch sequences (pipelines) of keygen, sign and verify.
+// One engine per process, bound to one device.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/params.h"
+#include "family_ops.h"
+
+namespace xb {
+
+struct LeafRef;
+struct TreeJob;
+
+class CudaFailure : public std::runtime_error {
+   public:
+    using std::runtime_error::runtime_error;
+};
+
+#define XB_CUDA(call)                                                                             \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            throw ::xb::CudaFailure(std::string(#call) + ": " + cudaGetErrorString(e_) + " at " + \
+                                    __FILE__ + ":" + std::to_string(__LINE__));                   \
+    } while (0)
+
+// Device buffer that only grows.  Growing waits for all device work.
+class DevBuf {
+   public:
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf();
+    void* get(size_t bytes);
+    template <class T>
+    T* as(size_t count)
+    {
+        return (T*)get(count * sizeof(T));
+    }
+
+   private:
+    void* p_ = nullptr;
+    size_t cap_ = 0;
+};
+
+// Pinned host buffer that only grows.
+class PinnedBuf {
+   public:
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+    ~PinnedBuf();
+    void* get(size_t bytes);
+    template <class T>
+    T* as(size_t count)
+    {
+        return (T*)get(count * sizeof(T));
+    }
+
+   private:
+    void* p_ = nullptr;
+    size_t cap_ = 0;
+};
+
+class Engine {
+   public:
+    static Engine& get();  // lazily created on the current device
+    explicit Engine(int device);
+    ~Engine();
+
+    std::mutex mu;  // serialises host-buffer calls
+
+    // Orders work on `st` after the previous call (scratch reuse) and records
+    // the end of this call's work.
+    void begin(cudaStream_t st);
+    void end(cudaStream_t st);
+
+    cudaStream_t stream() const { return stream_; }
+    int device() const { return device_; }
+
+    // -- pipelines (device pointers, asynchronous on st) ---------------------
+    // Builds every subtree of `jobs` (all of height h): node arrays at
+    // d_nodes + job.node_off, levels 0..h.  d_jobs is the device copy of jobs.
+    void build_trees(const FamilyOps* ops, const TreeJob* d_jobs, uint32_t njobs, int h, uint8_t* d_nodes,
+                     const void* d_ctx, cudaStream_t st);
+
+    // Verify of `count` signed messages against npk public keys (root||seed).
+    void verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_sm,
+                const uint64_t* d_sm_off, const uint64_t* d_smlen, const uint8_t* d_pk, uint32_t npk,
+                const uint32_t* d_pk_index, int* d_status, cudaStream_t st);
+
+    // Key generation from seeds (count x 3n) into pk (count x 2n) and sk
+    // (count x sk_bytes), no OID prefix.
+    void keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_seeds, uint8_t* d_pk,
+                 uint8_t* d_sk, cudaStream_t st);
+
+    // Signing given per-request key material.  h_sk: count x sk_bytes (no
+    // OID), already reflecting the reference's exhaustion handling; h_idx:
+    // the index each request signs with.  d_sm: output buffers with the
+    // message already at sm_off + sig_bytes.
+    void sign(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* h_sk,
+              const uint64_t* h_idx, uint8_t* d_sm, const uint64_t* d_sm_off, const uint64_t* d_mlen,
+              cudaStream_t st);
+
+    void core_hash(const FamilyOps* ops, uint32_t count, const uint8_t* d_in, const uint64_t* d_off,
+                   const uint64_t* d_len, uint8_t* d_out, cudaStream_t st);
+
+    // Work counters of the last verify (see xmss_b200_last_verify_work).
+    void last_verify_work(unsigned long long out[3]);
+
+    // Phase timing (xmss_b200_profile / xmss_b200_phase_ms).
+    enum Phase { kPrep = 0, kChains = 1, kLtree = 2, kRoot = 3, kTree = 4, kPhases = 5 };
+    bool profiling = false;
+    void mark(int phase, bool start, cudaStream_t st);  // no-op unless profiling
+    void phase_ms(double out[kPhases]);
+
+    // Scratch for host-buffer entry points (guarded by mu).
+    DevBuf d_in, d_in2, d_off, d_len, d_out, d_aux, d_aux2;
+    PinnedBuf h_stage, h_stage2;
+
+   private:
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t done_ = nullptr;
+    bool have_done_ = false;
+    // pipeline scratch
+    DevBuf s_ctx_, s_jobs_, s_refs_, s_wpk_, s_wpk2_, s_nodes_, s_keys_, s_node_, s_lens_, s_idx_, s_leaf_,
+        s_work_, s_tree_off_, s_key_idx_, s_mlen_;
+    PinnedBuf h_jobs_;
+    unsigned long long* work_ = nullptr;
+    struct Mark {
+        int phase;
+        cudaEvent_t a, b;
+    };
+    std::vector<Mark> marks_;
+    std::vector<cudaEvent_t> free_events_;
+    cudaEvent_t event();
+};
+
+// Engine selected by (func, n); throws when the family is not built.
+const FamilyOps* ops_for(const xmss_params& p);
+
+// rate_kernel.cu
+void launch_rate(int kind, uint32_t blocks, uint32_t iters, uint32_t* sink, cudaStream_t st);
+
+}  // namespace xb

@@ -1,0 +1,737 @@
+// Tweakable hash families of XMSS (the reference's hash.c), one struct per
+// (hash function, n) pair that the parameter tables can select
+// (cuxmss/hash.c:29-65 core_hash dispatch):
+//
+//   Sha256N32   SHA-256,        n = 32, padding_len = 32   (midstate form)
+//   Sha512N64   SHA-512,        n = 64, padding_len = 64   (midstate form)
+//   Sha256N24   SHA-256 / 24 B, n = 24, padding_len = 4
+//   Shake128N32 SHAKE128,       n = 32, padding_len = 32
+//   Shake256N24 / N32 / N64     SHAKE256, padding_len = 4 / 32 / 64
+//
+// Every family exposes the same interface over n-byte values held as NW
+// 32-bit words in the family's message-word order (big-endian words for
+// SHA-2, little-endian words for Keccak):
+//   Ctx                 per-key precomputation (seeds, midstates)
+//   make_ctx            builds it from PUB_SEED, SK_SEED, SK_PRF
+//   load / store        bytes <-> words
+//   thash_f, thash_h    hash.c:157-183, 125-155 (ADRS word 7 is overwritten)
+//   prf_keygen          hash.c:87-98 with in = PUB_SEED || ADRS
+//   prf_r               hash.c:70-81 with key = SK_PRF, in = toByte(idx, 32)
+//   hmsg                hash.c:107-120 over a message in global memory
+//   byte_at             byte k of an n-byte value (for base_w)
+//
+// For the SHA-2 sets with padding_len = n the first block of PRF, PRF_keygen
+// and the R-PRF is toByte(X, n) || key and is constant per key, so its
+// compression is done once per key ("midstate"); F then costs 4 and H 6
+// compressions instead of 6 and 9.
+#pragma once
+
+#include <cstdint>
+
+#include "hashcore.cuh"
+
+namespace xb {
+
+// ---------------------------------------------------------------------------
+// Byte access helpers.
+// ---------------------------------------------------------------------------
+
+// Four message bytes starting at offset o (zero past mlen), packed
+// little-endian (byte o in bits 0..7).  Uses two aligned word loads when the
+// whole aligned pair lies inside [m, m + mlen); callers guarantee that the
+// 3 bytes before m are readable (m is 4-byte aligned, or preceded by the
+// signature in an sm buffer).
+__device__ __forceinline__ uint32_t fetch4_le(const uint8_t* m, uint64_t mlen, uint64_t o)
+{
+    if (o + 8 <= mlen) {
+        const uintptr_t addr = (uintptr_t)(m + o);
+        const uint32_t* a = (const uint32_t*)(addr & ~(uintptr_t)3);
+        const int sh = (int)(addr & 3) * 8;
+        const uint32_t lo = __ldg(a);
+        if (!sh) return lo;
+        return __funnelshift_r(lo, __ldg(a + 1), sh);
+    }
+    uint32_t v = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        if (o + i < mlen) v |= (uint32_t)__ldg(m + o + i) << (8 * i);
+    return v;
+}
+
+// NW little-endian words from bytes at p (any alignment).
+template <int NW>
+__device__ __forceinline__ void load_le(uint32_t (&v)[NW], const uint8_t* p)
+{
+    if (((uintptr_t)p & 3) == 0) {
+#pragma unroll
+        for (int i = 0; i < NW; i++) v[i] = ((const uint32_t*)p)[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < NW; i++)
+            v[i] = (uint32_t)p[4 * i] | ((uint32_t)p[4 * i + 1] << 8) |
+                   ((uint32_t)p[4 * i + 2] << 16) | ((uint32_t)p[4 * i + 3] << 24);
+    }
+}
+
+template <int NW>
+__device__ __forceinline__ void store_le(uint8_t* p, const uint32_t (&v)[NW])
+{
+    if (((uintptr_t)p & 15) == 0 && NW % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < NW; i += 4)
+            *(uint4*)(p + 4 * i) = make_uint4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+    } else if (((uintptr_t)p & 3) == 0) {
+#pragma unroll
+        for (int i = 0; i < NW; i++) ((uint32_t*)p)[i] = v[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < NW; i++) {
+            p[4 * i] = (uint8_t)v[i];
+            p[4 * i + 1] = (uint8_t)(v[i] >> 8);
+            p[4 * i + 2] = (uint8_t)(v[i] >> 16);
+            p[4 * i + 3] = (uint8_t)(v[i] >> 24);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Shared pieces of every family.
+// ---------------------------------------------------------------------------
+template <int N_, int PL_, bool BE_>
+struct FamBase {
+    static constexpr int N = N_;
+    static constexpr int NW = N_ / 4;
+    static constexpr int PL = PL_;   // padding_len
+    static constexpr int PW = PL_ / 4;
+    static constexpr int LEN1 = 2 * N_;  // w = 16
+    static constexpr int LEN2 = 3;
+    static constexpr int LEN = LEN1 + LEN2;
+    static constexpr bool BE = BE_;
+
+    // Message word for a big-endian u32 value (ADRS words, toByte fields).
+    __device__ __forceinline__ static uint32_t mw(uint32_t x) { return BE ? x : bswap32(x); }
+
+    __device__ __forceinline__ static void load(uint32_t (&v)[NW], const uint8_t* p)
+    {
+        load_le<NW>(v, p);
+        if (BE) {
+#pragma unroll
+            for (int i = 0; i < NW; i++) v[i] = bswap32(v[i]);
+        }
+    }
+    __device__ __forceinline__ static void store(uint8_t* p, const uint32_t (&v)[NW])
+    {
+        if (BE) {
+            uint32_t t[NW];
+#pragma unroll
+            for (int i = 0; i < NW; i++) t[i] = bswap32(v[i]);
+            store_le<NW>(p, t);
+        } else {
+            store_le<NW>(p, v);
+        }
+    }
+    __device__ __forceinline__ static uint32_t byte_at(const uint32_t (&v)[NW], int k)
+    {
+        const uint32_t w = v[k >> 2];
+        return BE ? (w >> (24 - 8 * (k & 3))) & 0xFF : (w >> (8 * (k & 3))) & 0xFF;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Generic family: every call hashes an explicit word message with core().
+// ---------------------------------------------------------------------------
+template <class Core, int N_, int PL_>
+struct GenericFam : FamBase<N_, PL_, Core::BE> {
+    using B = FamBase<N_, PL_, Core::BE>;
+    using B::mw;
+    static constexpr int NW = B::NW, PW = B::PW;
+
+    struct Ctx {
+        uint32_t pub[NW];
+        uint32_t sks[NW];
+        uint32_t skp[NW];
+    };
+
+    __device__ static void make_ctx(Ctx& c, const uint8_t* pub, const uint8_t* sks, const uint8_t* skp)
+    {
+        B::load(c.pub, pub);
+#pragma unroll
+        for (int i = 0; i < NW; i++) c.sks[i] = c.skp[i] = 0;
+        if (sks) B::load(c.sks, sks);
+        if (skp) B::load(c.skp, skp);
+    }
+
+    template <int MW>
+    __device__ __forceinline__ static void set_pad(uint32_t (&m)[MW], uint32_t x)
+    {
+#pragma unroll
+        for (int i = 0; i < PW - 1; i++) m[i] = 0;
+        m[PW - 1] = mw(x);
+    }
+
+    // PRF(PUB_SEED, ADRS), hash.c:70-81
+    __device__ __forceinline__ static void prf_adrs(uint32_t (&out)[NW], const Ctx& c, const uint32_t (&a)[8])
+    {
+        uint32_t m[PW + NW + 8];
+        set_pad(m, 3);
+#pragma unroll
+        for (int i = 0; i < NW; i++) m[PW + i] = c.pub[i];
+#pragma unroll
+        for (int i = 0; i < 8; i++) m[PW + NW + i] = mw(a[i]);
+        Core::template digest<PW + NW + 8, NW>(out, m);
+    }
+
+    __device__ static void thash_f(uint32_t (&x)[NW], const Ctx& c, uint32_t (&a)[8])
+    {
+        uint32_t m[PW + 2 * NW], mask[NW], key[NW];
+        a[7] = 0;
+        prf_adrs(key, c, a);
+        a[7] = 1;
+        prf_adrs(mask, c, a);
+        set_pad(m, 0);
+#pragma unroll
+        for (int i = 0; i < NW; i++) {
+            m[PW + i] = key[i];
+            m[PW + NW + i] = x[i] ^ mask[i];
+        }
+        Core::template digest<PW + 2 * NW, NW>(x, m);
+    }
+
+    __device__ static void thash_h(uint32_t (&o)[NW], const uint32_t (&l)[NW], const uint32_t (&r)[NW],
+                                   const Ctx& c, uint32_t (&a)[8])
+    {
+        uint32_t m[PW + 3 * NW], t[NW];
+        set_pad(m, 1);
+        a[7] = 0;
+        prf_adrs(t, c, a);
+#pragma unroll
+        for (int i = 0; i < NW; i++) m[PW + i] = t[i];
+        a[7] = 1;
+        prf_adrs(t, c, a);
+#pragma unroll
+        for (int i = 0; i < NW; i++) m[PW + NW + i] = l[i] ^ t[i];
+        a[7] = 2;
+        prf_adrs(t, c, a);
+#pragma unroll
+        for (int i = 0; i < NW; i++) m[PW + 2 * NW + i] = r[i] ^ t[i];
+        Core::template digest<PW + 3 * NW, NW>(o, m);
+    }
+
+    __device__ static void prf_keygen(uint32_t (&o)[NW], const Ctx& c, const uint32_t (&a)[8])
+    {
+        uint32_t m[PW + 2 * NW + 8];
+        set_pad(m, 4);
+#pragma unroll
+        for (int i = 0; i < NW; i++) {
+            m[PW + i] = c.sks[i];
+            m[PW + NW + i] = c.pub[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) m[PW + 2 * NW + i] = mw(a[i]);
+        Core::template digest<PW + 2 * NW + 8, NW>(o, m);
+    }
+
+    __device__ static void prf_r(uint32_t (&o)[NW], const Ctx& c, uint64_t idx)
+    {
+        uint32_t m[PW + NW + 8];
+        set_pad(m, 3);
+#pragma unroll
+        for (int i = 0; i < NW; i++) m[PW + i] = c.skp[i];
+#pragma unroll
+        for (int i = 0; i < 6; i++) m[PW + NW + i] = 0;
+        m[PW + NW + 6] = mw((uint32_t)(idx >> 32));
+        m[PW + NW + 7] = mw((uint32_t)idx);
+        Core::template digest<PW + NW + 8, NW>(o, m);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Core hash adaptors for GenericFam.
+// ---------------------------------------------------------------------------
+struct CoreSha256 {
+    static constexpr bool BE = true;
+    template <int MW, int OW>
+    __device__ __forceinline__ static void digest(uint32_t (&out)[OW], const uint32_t (&m)[MW])
+    {
+        uint32_t full[8];
+        sha256_words<MW>(full, m);
+#pragma unroll
+        for (int i = 0; i < OW; i++) out[i] = full[i];  // n = 24 truncates (hash.c:35-38)
+    }
+};
+
+template <int RATEW>
+struct CoreShake {
+    static constexpr bool BE = false;
+    template <int MW, int OW>
+    __device__ __forceinline__ static void digest(uint32_t (&out)[OW], const uint32_t (&m)[MW])
+    {
+        shake_words<RATEW, MW, OW>(out, m);
+    }
+};
+
+using Sha256N24 = GenericFam<CoreSha256, 24, 4>;
+using Shake128N32 = GenericFam<CoreShake<42>, 32, 32>;
+using Shake256N24 = GenericFam<CoreShake<34>, 24, 4>;
+using Shake256N32 = GenericFam<CoreShake<34>, 32, 32>;
+using Shake256N64 = GenericFam<CoreShake<34>, 64, 64>;
+
+// ---------------------------------------------------------------------------
+// SHA-256, n = 32, padding_len = 32: midstate form.
+// ---------------------------------------------------------------------------
+struct Sha256N32 : FamBase<32, 32, true> {
+    struct Ctx {
+        uint32_t pub[8];
+        uint32_t sks[8];
+        uint32_t prf_mid[8];  // compress(IV, toByte(3,32) || PUB_SEED)
+        uint32_t kg_mid[8];   // compress(IV, toByte(4,32) || SK_SEED)
+        uint32_t r_mid[8];    // compress(IV, toByte(3,32) || SK_PRF)
+    };
+
+    __device__ __forceinline__ static void mid(uint32_t (&st)[8], uint32_t x, const uint32_t (&k)[8])
+    {
+        uint32_t w[16];
+#pragma unroll
+        for (int i = 0; i < 7; i++) w[i] = 0;
+        w[7] = x;
+#pragma unroll
+        for (int i = 0; i < 8; i++) w[8 + i] = k[i];
+        sha256_iv(st);
+        sha256_compress(st, w);
+    }
+
+    __device__ static void make_ctx(Ctx& c, const uint8_t* pub, const uint8_t* sks, const uint8_t* skp)
+    {
+        uint32_t t[8];
+        load(c.pub, pub);
+        mid(c.prf_mid, 3, c.pub);
+#pragma unroll
+        for (int i = 0; i < 8; i++) c.sks[i] = 0;
+        if (sks) load(c.sks, sks);
+        mid(c.kg_mid, 4, c.sks);
+#pragma unroll
+        for (int i = 0; i < 8; i++) t[i] = 0;
+        if (skp) load(t, skp);
+        mid(c.r_mid, 3, t);
+    }
+
+    // PRF(PUB_SEED, ADRS): one compression from the PRF midstate.
+    __device__ __forceinline__ static void prf_adrs(uint32_t (&out)[8], const Ctx& c, const uint32_t (&a)[8])
+    {
+        uint32_t w[16];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            w[i] = a[i];
+            out[i] = c.prf_mid[i];
+        }
+        w[8] = 0x80000000u;
+#pragma unroll
+        for (int i = 9; i < 15; i++) w[i] = 0;
+        w[15] = 768;
+        sha256_compress(out, w);
+    }
+
+    __device__ static void thash_f(uint32_t (&x)[8], const Ctx& c, uint32_t (&a)[8])
+    {
+        uint32_t key[8], t[8], w[16];
+        a[7] = 1;
+        prf_adrs(t, c, a);  // mask
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] ^= t[i];
+        a[7] = 0;
+        prf_adrs(key, c, a);
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            w[i] = 0;
+            w[8 + i] = key[i];
+        }
+        sha256_iv(t);
+        sha256_compress(t, w);
+#pragma unroll
+        for (int i = 0; i < 8; i++) w[i] = x[i];
+        w[8] = 0x80000000u;
+#pragma unroll
+        for (int i = 9; i < 15; i++) w[i] = 0;
+        w[15] = 768;
+        sha256_compress(t, w);
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = t[i];
+    }
+
+    __device__ static void thash_h(uint32_t (&o)[8], const uint32_t (&l)[8], const uint32_t (&r)[8],
+                                   const Ctx& c, uint32_t (&a)[8])
+    {
+        uint32_t t[8], st[8], w[16];
+        a[7] = 0;
+        prf_adrs(t, c, a);  // key
+#pragma unroll
+        for (int i = 0; i < 7; i++) w[i] = 0;
+        w[7] = 1;
+#pragma unroll
+        for (int i = 0; i < 8; i++) w[8 + i] = t[i];
+        sha256_iv(st);
+        sha256_compress(st, w);
+        a[7] = 1;
+        prf_adrs(t, c, a);
+#pragma unroll
+        for (int i = 0; i < 8; i++) w[i] = l[i] ^ t[i];
+        a[7] = 2;
+        prf_adrs(t, c, a);
+#pragma unroll
+        for (int i = 0; i < 8; i++) w[8 + i] = r[i] ^ t[i];
+        sha256_compress(st, w);
+        w[0] = 0x80000000u;
+#pragma unroll
+        for (int i = 1; i < 15; i++) w[i] = 0;
+        w[15] = 1024;
+        sha256_compress(st, w);
+#pragma unroll
+        for (int i = 0; i < 8; i++) o[i] = st[i];
+    }
+
+    __device__ static void prf_keygen(uint32_t (&o)[8], const Ctx& c, const uint32_t (&a)[8])
+    {
+        uint32_t w[16];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            w[i] = c.pub[i];
+            w[8 + i] = a[i];
+            o[i] = c.kg_mid[i];
+        }
+        sha256_compress(o, w);
+        w[0] = 0x80000000u;
+#pragma unroll
+        for (int i = 1; i < 15; i++) w[i] = 0;
+        w[15] = 1024;
+        sha256_compress(o, w);
+    }
+
+    __device__ static void prf_r(uint32_t (&o)[8], const Ctx& c, uint64_t idx)
+    {
+        uint32_t w[16];
+#pragma unroll
+        for (int i = 0; i < 6; i++) w[i] = 0;
+        w[6] = (uint32_t)(idx >> 32);
+        w[7] = (uint32_t)idx;
+        w[8] = 0x80000000u;
+#pragma unroll
+        for (int i = 9; i < 15; i++) w[i] = 0;
+        w[15] = 768;
+#pragma unroll
+        for (int i = 0; i < 8; i++) o[i] = c.r_mid[i];
+        sha256_compress(o, w);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// SHA-512, n = 64, padding_len = 64: midstate form over 64-bit words.
+// ---------------------------------------------------------------------------
+struct Sha512N64 : FamBase<64, 64, true> {
+    struct Ctx {
+        uint32_t pub[16];
+        uint32_t sks[16];
+        uint64_t prf_mid[8];
+        uint64_t kg_mid[8];
+        uint64_t r_mid[8];
+    };
+
+    __device__ __forceinline__ static void mid(uint64_t (&st)[8], uint64_t x, const uint32_t (&k)[16])
+    {
+        uint64_t w[16];
+#pragma unroll
+        for (int i = 0; i < 7; i++) w[i] = 0;
+        w[7] = x;
+#pragma unroll
+        for (int i = 0; i < 8; i++) w[8 + i] = join64(k[2 * i], k[2 * i + 1]);
+        sha512_iv(st);
+        sha512_compress(st, w);
+    }
+
+    __device__ __forceinline__ static void out16(uint32_t (&o)[16], const uint64_t (&st)[8])
+    {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            o[2 * i] = (uint32_t)(st[i] >> 32);
+            o[2 * i + 1] = (uint32_t)st[i];
+        }
+    }
+
+    __device__ static void make_ctx(Ctx& c, const uint8_t* pub, const uint8_t* sks, const uint8_t* skp)
+    {
+        uint32_t t[16];
+        load(c.pub, pub);
+        mid(c.prf_mid, 3, c.pub);
+#pragma unroll
+        for (int i = 0; i < 16; i++) c.sks[i] = 0;
+        if (sks) load(c.sks, sks);
+        mid(c.kg_mid, 4, c.sks);
+#pragma unroll
+        for (int i = 0; i < 16; i++) t[i] = 0;
+        if (skp) load(t, skp);
+        mid(c.r_mid, 3, t);
+    }
+
+    __device__ __forceinline__ static void prf_adrs(uint64_t (&st)[8], const Ctx& c, const uint32_t (&a)[8])
+    {
+        uint64_t w[16];
+#pragma unroll
+        for (int i = 0; i < 4; i++) w[i] = join64(a[2 * i], a[2 * i + 1]);
+        w[4] = 0x8000000000000000ull;
+#pragma unroll
+        for (int i = 5; i < 15; i++) w[i] = 0;
+        w[15] = 1280;  // (64 + 64 + 32) * 8
+#pragma unroll
+        for (int i = 0; i < 8; i++) st[i] = c.prf_mid[i];
+        sha512_compress(st, w);
+    }
+
+    __device__ static void thash_f(uint32_t (&x)[16], const Ctx& c, uint32_t (&a)[8])
+    {
+        uint64_t t[8], st[8], w[16];
+        a[7] = 0;
+        prf_adrs(t, c, a);  // key
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            w[i] = 0;
+            w[8 + i] = t[i];
+        }
+        sha512_iv(st);
+        sha512_compress(st, w);
+        a[7] = 1;
+        prf_adrs(t, c, a);  // mask
+#pragma unroll
+        for (int i = 0; i < 8; i++) w[i] = join64(x[2 * i], x[2 * i + 1]) ^ t[i];
+        w[8] = 0x8000000000000000ull;
+#pragma unroll
+        for (int i = 9; i < 15; i++) w[i] = 0;
+        w[15] = 1536;  // 192 * 8
+        sha512_compress(st, w);
+        out16(x, st);
+    }
+
+    __device__ static void thash_h(uint32_t (&o)[16], const uint32_t (&l)[16], const uint32_t (&r)[16],
+                                   const Ctx& c, uint32_t (&a)[8])
+    {
+        uint64_t t[8], st[8], w[16];
+        a[7] = 0;
+        prf_adrs(t, c, a);
+#pragma unroll
+        for (int i = 0; i < 7; i++) w[i] = 0;
+        w[7] = 1;
+#pragma unroll
+        for (int i = 0; i < 8; i++) w[8 + i] = t[i];
+        sha512_iv(st);
+        sha512_compress(st, w);
+        a[7] = 1;
+        prf_adrs(t, c, a);
+#pragma unroll
+        for (int i = 0; i < 8; i++) w[i] = join64(l[2 * i], l[2 * i + 1]) ^ t[i];
+        a[7] = 2;
+        prf_adrs(t, c, a);
+#pragma unroll
+        for (int i = 0; i < 8; i++) w[8 + i] = join64(r[2 * i], r[2 * i + 1]) ^ t[i];
+        sha512_compress(st, w);
+        w[0] = 0x8000000000000000ull;
+#pragma unroll
+        for (int i = 1; i < 15; i++) w[i] = 0;
+        w[15] = 2048;  // 256 * 8
+        sha512_compress(st, w);
+        out16(o, st);
+    }
+
+    __device__ static void prf_keygen(uint32_t (&o)[16], const Ctx& c, const uint32_t (&a)[8])
+    {
+        uint64_t st[8], w[16];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            w[i] = join64(c.pub[2 * i], c.pub[2 * i + 1]);
+            st[i] = c.kg_mid[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) w[8 + i] = join64(a[2 * i], a[2 * i + 1]);
+        w[12] = 0x8000000000000000ull;
+        w[13] = 0;
+        w[14] = 0;
+        w[15] = 1792;  // (64 + 64 + 64 + 32) * 8
+        sha512_compress(st, w);
+        out16(o, st);
+    }
+
+    __device__ static void prf_r(uint32_t (&o)[16], const Ctx& c, uint64_t idx)
+    {
+        uint64_t st[8], w[16];
+        w[0] = 0;
+        w[1] = 0;
+        w[2] = 0;
+        w[3] = idx;
+        w[4] = 0x8000000000000000ull;
+#pragma unroll
+        for (int i = 5; i < 15; i++) w[i] = 0;
+        w[15] = 1280;
+#pragma unroll
+        for (int i = 0; i < 8; i++) st[i] = c.r_mid[i];
+        sha512_compress(st, w);
+        out16(o, st);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// H_msg (hash.c:107-120): toByte(2, pl) || R || root || toByte(idx, n) || M,
+// streamed block by block from global memory.  One thread per message.
+// ---------------------------------------------------------------------------
+template <class F>
+struct HMsgPrefix {
+    static constexpr int W = F::PW + 3 * F::NW;  // prefix words
+    uint32_t w[W];
+    __device__ __forceinline__ void build(const uint32_t (&R)[F::NW], const uint32_t (&root)[F::NW], uint64_t idx)
+    {
+#pragma unroll
+        for (int i = 0; i < F::PW - 1; i++) w[i] = 0;
+        w[F::PW - 1] = F::mw(2);
+#pragma unroll
+        for (int i = 0; i < F::NW; i++) {
+            w[F::PW + i] = R[i];
+            w[F::PW + F::NW + i] = root[i];
+            w[F::PW + 2 * F::NW + i] = 0;
+        }
+        w[W - 1] = F::mw((uint32_t)idx);
+        w[W - 2] = F::mw((uint32_t)(idx >> 32));
+    }
+};
+
+// Stream word k (4 bytes at offset 4k) of prefix || M as a little-endian
+// packed value.
+template <class F>
+__device__ __forceinline__ uint32_t stream_le(const HMsgPrefix<F>& pre, const uint8_t* m, uint64_t mlen, uint64_t k)
+{
+    if (k < (uint64_t)HMsgPrefix<F>::W) {
+        const uint32_t v = pre.w[k];
+        return F::BE ? bswap32(v) : v;
+    }
+    return fetch4_le(m, mlen, 4 * (k - HMsgPrefix<F>::W));
+}
+
+// SHA-256 / SHA-512 / SHAKE streaming over the padded message.
+template <class F, int KIND>  // KIND 0 = SHA-256, 1 = SHA-512, 2 = SHAKE (rate from F)
+struct HMsgImpl;
+
+template <class F>
+struct HMsgImpl<F, 0> {
+    __device__ static void run(uint32_t (&out)[F::NW], const HMsgPrefix<F>& pre, const uint8_t* m, uint64_t mlen)
+    {
+        const uint64_t L = 4ull * HMsgPrefix<F>::W + mlen;
+        const uint64_t nb = (L + 9 + 63) / 64;
+        uint32_t st[8];
+        sha256_iv(st);
+        for (uint64_t b = 0; b < nb; b++) {
+            uint32_t w[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                const uint64_t o = 64 * b + 4 * j;  // byte offset of this word
+                uint32_t le = (o < L) ? stream_le<F>(pre, m, mlen, o >> 2) : 0;
+                if (o <= L && L < o + 4) le |= 0x80u << (8 * (L - o));
+                w[j] = bswap32(le);
+            }
+            if (b == nb - 1) {
+                w[14] = (uint32_t)((L * 8) >> 32);
+                w[15] = (uint32_t)(L * 8);
+            }
+            sha256_compress(st, w);
+        }
+#pragma unroll
+        for (int i = 0; i < F::NW; i++) out[i] = st[i];
+    }
+};
+
+template <class F>
+struct HMsgImpl<F, 1> {
+    __device__ static void run(uint32_t (&out)[F::NW], const HMsgPrefix<F>& pre, const uint8_t* m, uint64_t mlen)
+    {
+        const uint64_t L = 4ull * HMsgPrefix<F>::W + mlen;
+        const uint64_t nb = (L + 17 + 127) / 128;
+        uint64_t st[8];
+        sha512_iv(st);
+        for (uint64_t b = 0; b < nb; b++) {
+            uint64_t w[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                uint32_t hl[2];
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    const uint64_t o = 128 * b + 8 * j + 4 * q;
+                    uint32_t le = (o < L) ? stream_le<F>(pre, m, mlen, o >> 2) : 0;
+                    if (o <= L && L < o + 4) le |= 0x80u << (8 * (L - o));
+                    hl[q] = bswap32(le);
+                }
+                w[j] = join64(hl[0], hl[1]);
+            }
+            if (b == nb - 1) {
+                w[14] = 0;
+                w[15] = L * 8;
+            }
+            sha512_compress(st, w);
+        }
+        uint32_t o16[16];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            o16[2 * i] = (uint32_t)(st[i] >> 32);
+            o16[2 * i + 1] = (uint32_t)st[i];
+        }
+#pragma unroll
+        for (int i = 0; i < F::NW; i++) out[i] = o16[i];
+    }
+};
+
+template <class F, int RATEW>
+__device__ void hmsg_shake(uint32_t (&out)[F::NW], const HMsgPrefix<F>& pre, const uint8_t* m, uint64_t mlen)
+{
+    const uint64_t L = 4ull * HMsgPrefix<F>::W + mlen;
+    const uint64_t RB = 4 * RATEW;
+    const uint64_t nb = L / RB + 1;
+    uint64_t A[25];
+#pragma unroll
+    for (int i = 0; i < 25; i++) A[i] = 0;
+    for (uint64_t b = 0; b < nb; b++) {
+#pragma unroll
+        for (int i = 0; i < RATEW / 2; i++) {
+            uint32_t hl[2];
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const uint64_t o = RB * b + 8 * i + 4 * q;
+                uint32_t le = (o < L) ? stream_le<F>(pre, m, mlen, o >> 2) : 0;
+                if (o <= L && L < o + 4) le ^= 0x1Fu << (8 * (L - o));
+                hl[q] = le;
+            }
+            if (b == nb - 1 && 2 * i + 1 == RATEW - 1) hl[1] ^= 0x80000000u;
+            A[i] ^= ((uint64_t)hl[1] << 32) | hl[0];
+        }
+        keccak_f1600(A);
+    }
+#pragma unroll
+    for (int i = 0; i < F::NW; i++) out[i] = (i & 1) ? (uint32_t)(A[i / 2] >> 32) : (uint32_t)A[i / 2];
+}
+
+template <class F> struct HMsgKind;
+template <> struct HMsgKind<Sha256N32> { static constexpr int v = 0; };
+template <> struct HMsgKind<Sha256N24> { static constexpr int v = 0; };
+template <> struct HMsgKind<Sha512N64> { static constexpr int v = 1; };
+template <> struct HMsgKind<Shake128N32> { static constexpr int v = 42; };
+template <> struct HMsgKind<Shake256N24> { static constexpr int v = 34; };
+template <> struct HMsgKind<Shake256N32> { static constexpr int v = 34; };
+template <> struct HMsgKind<Shake256N64> { static constexpr int v = 34; };
+
+template <class F>
+__device__ void hmsg(uint32_t (&out)[F::NW], const uint32_t (&R)[F::NW], const uint32_t (&root)[F::NW],
+                     uint64_t idx, const uint8_t* m, uint64_t mlen)
+{
+    HMsgPrefix<F> pre;
+    pre.build(R, root, idx);
+    constexpr int K = HMsgKind<F>::v;
+    if constexpr (K == 0 || K == 1) {
+        HMsgImpl<F, K>::run(out, pre, m, mlen);
+    } else {
+        hmsg_shake<F, K>(out, pre, m, mlen);
+    }
+}
+
+}  // namespace xb

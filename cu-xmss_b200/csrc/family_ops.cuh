@@ -1,0 +1,93 @@
+// Launchers that bind the templated kernels of one family into a FamilyOps
+// table.  Included by exactly one fam_*.cu per family.
+#pragma once
+
+#include "family_ops.h"
+#include "xmss_kernels.cuh"
+
+namespace xb {
+
+constexpr int kBlock = 128;
+
+inline unsigned grid_for(uint64_t items)
+{
+    return (unsigned)((items + kBlock - 1) / kBlock);
+}
+
+template <class F>
+struct Launch {
+    using Ctx = typename F::Ctx;
+
+    static void make_ctx(const uint8_t* pub, uint32_t pub_stride, const uint8_t* sks, uint32_t sks_stride,
+                         const uint8_t* skp, uint32_t skp_stride, uint32_t nkeys, void* ctx, cudaStream_t st)
+    {
+        if (!nkeys) return;
+        k_make_ctx<F><<<grid_for(nkeys), kBlock, 0, st>>>(pub, pub_stride, sks, sks_stride, skp, skp_stride, nkeys,
+                                                          (Ctx*)ctx);
+    }
+    static void keygen_chains(const TreeJob* jobs, int h, uint64_t slot0, uint64_t nslots, const void* ctx,
+                              uint8_t* wpk, LeafRef* refs, cudaStream_t st)
+    {
+        const uint64_t items = nslots * F::LEN;
+        if (!items) return;
+        k_keygen_chains<F><<<grid_for(items), kBlock, 0, st>>>(jobs, h, slot0, nslots, (const Ctx*)ctx, wpk, refs);
+    }
+    static void ltree_level(const LeafRef* refs, uint32_t nslots, int level, int cnt_in, const uint8_t* src,
+                            uint32_t src_stride, uint8_t* dst, uint32_t dst_stride, uint8_t* leaf_out,
+                            const void* ctx, const int* status, cudaStream_t st)
+    {
+        const uint64_t items = (uint64_t)nslots * ((cnt_in + 1) / 2);
+        if (!items) return;
+        k_ltree_level<F><<<grid_for(items), kBlock, 0, st>>>(refs, nslots, level, cnt_in, src, src_stride, dst,
+                                                              dst_stride, leaf_out, (const Ctx*)ctx, status);
+    }
+    static void tree_level(const TreeJob* jobs, uint32_t njobs, int h, int level, uint8_t* nodes, const void* ctx,
+                           cudaStream_t st)
+    {
+        const uint64_t items = (uint64_t)njobs << (h - level - 1);
+        if (!items) return;
+        k_tree_level<F><<<grid_for(items), kBlock, 0, st>>>(jobs, njobs, h, level, nodes, (const Ctx*)ctx);
+    }
+    static void verify_prep(const VerifyArgs& v, const void* ctx, cudaStream_t st)
+    {
+        if (!v.count) return;
+        k_verify_prep<F><<<grid_for(v.count), 64, 0, st>>>(v, (const Ctx*)ctx);
+    }
+    static void verify_chains(const VerifyArgs& v, uint32_t layer, const void* ctx, cudaStream_t st)
+    {
+        const uint64_t items = (uint64_t)v.count * F::LEN;
+        if (!items) return;
+        k_verify_chains<F><<<grid_for(items), kBlock, 0, st>>>(v, layer, (const Ctx*)ctx);
+    }
+    static void verify_root(const VerifyArgs& v, uint32_t layer, const void* ctx, cudaStream_t st)
+    {
+        if (!v.count) return;
+        k_verify_root<F><<<(v.count + 63) / 64, 64, 0, st>>>(v, layer, (const Ctx*)ctx);
+    }
+    static void sign_prep(const SignArgs& g, const void* ctx, cudaStream_t st)
+    {
+        if (!g.count) return;
+        k_sign_prep<F><<<(g.count + 63) / 64, 64, 0, st>>>(g, (const Ctx*)ctx);
+    }
+    static void sign_chains(const SignArgs& g, const void* ctx, cudaStream_t st)
+    {
+        const uint64_t items = (uint64_t)g.count * g.d * F::LEN;
+        if (!items) return;
+        k_sign_chains<F><<<grid_for(items), kBlock, 0, st>>>(g, (const Ctx*)ctx);
+    }
+    static void core_hash(const uint8_t* msgs, const uint64_t* off, const uint64_t* len, uint32_t count,
+                          uint8_t* out, cudaStream_t st)
+    {
+        if (!count) return;
+        k_core_hash<F><<<(count + 63) / 64, 64, 0, st>>>(msgs, off, len, count, out);
+    }
+
+    static FamilyOps table(const char* name, unsigned func)
+    {
+        return FamilyOps{name,          func,          (unsigned)F::N, (unsigned)F::LEN, sizeof(Ctx),
+                         make_ctx,      keygen_chains, ltree_level,    tree_level,       verify_prep,
+                         verify_chains, verify_root,   sign_prep,      sign_chains,      core_hash};
+    }
+};
+
+}  // namespace xb

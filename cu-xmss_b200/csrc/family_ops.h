@@ -1,0 +1,50 @@
+// Host-side launch table of one hash family.  Each fam_*.cu translation
+// unit instantiates the kernels of xmss_kernels.cuh for its family and
+// fills one FamilyOps; the engine picks the table by (func, n).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace xb {
+
+struct LeafRef;
+struct TreeJob;
+struct VerifyArgs;
+struct SignArgs;
+
+struct FamilyOps {
+    const char* name;
+    unsigned func, n, len;
+    size_t ctx_bytes;  // sizeof(F::Ctx)
+    void (*make_ctx)(const uint8_t* pub, uint32_t pub_stride, const uint8_t* sks, uint32_t sks_stride,
+                     const uint8_t* skp, uint32_t skp_stride, uint32_t nkeys, void* ctx, cudaStream_t st);
+    void (*keygen_chains)(const TreeJob* jobs, int h, uint64_t slot0, uint64_t nslots, const void* ctx,
+                          uint8_t* wpk, LeafRef* refs, cudaStream_t st);
+    void (*ltree_level)(const LeafRef* refs, uint32_t nslots, int level, int cnt_in, const uint8_t* src,
+                        uint32_t src_stride, uint8_t* dst, uint32_t dst_stride, uint8_t* leaf_out, const void* ctx,
+                        const int* status, cudaStream_t st);
+    void (*tree_level)(const TreeJob* jobs, uint32_t njobs, int h, int level, uint8_t* nodes, const void* ctx,
+                       cudaStream_t st);
+    void (*verify_prep)(const VerifyArgs& v, const void* ctx, cudaStream_t st);
+    void (*verify_chains)(const VerifyArgs& v, uint32_t layer, const void* ctx, cudaStream_t st);
+    void (*verify_root)(const VerifyArgs& v, uint32_t layer, const void* ctx, cudaStream_t st);
+    void (*sign_prep)(const SignArgs& g, const void* ctx, cudaStream_t st);
+    void (*sign_chains)(const SignArgs& g, const void* ctx, cudaStream_t st);
+    void (*core_hash)(const uint8_t* msgs, const uint64_t* off, const uint64_t* len, uint32_t count, uint8_t* out,
+                      cudaStream_t st);
+};
+
+// nullptr when (func, n) has no instantiation.
+const FamilyOps* family_ops(unsigned func, unsigned n);
+
+extern const FamilyOps kOpsSha256N32;
+extern const FamilyOps kOpsSha256N24;
+extern const FamilyOps kOpsSha512N64;
+extern const FamilyOps kOpsShake128N32;
+extern const FamilyOps kOpsShake256N24;
+extern const FamilyOps kOpsShake256N32;
+extern const FamilyOps kOpsShake256N64;
+
+}  // namespace xb

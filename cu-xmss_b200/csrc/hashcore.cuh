@@ -1,0 +1,271 @@
+// Hash cores for sm_100a: SHA-256 and SHA-512 compressions (FIPS 180-4) and
+// Keccak-f[1600] (FIPS 202), all register resident and fully unrolled so that
+// round constants become immediates and rotates become funnel shifts.
+//
+// Messages are handled as arrays of 32-bit words whose count is a compile-time
+// constant; SHA-2 words are big-endian (word i = bytes 4i..4i+3, most
+// significant first), Keccak words are little-endian (lane = w[2i] | w[2i+1]<<32).
+#pragma once
+
+#include <cstdint>
+
+namespace xb {
+
+__device__ __forceinline__ uint32_t ror32(uint32_t x, int n) { return __funnelshift_r(x, x, n); }
+__device__ __forceinline__ uint32_t bswap32(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
+
+// ---------------------------------------------------------------------------
+// SHA-256 compression (FIPS 180-4 6.2.2).  `w` is consumed (message schedule
+// is expanded in place in a 16-word window).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void sha256_compress(uint32_t (&st)[8], uint32_t (&w)[16])
+{
+    const uint32_t K[64] = {
+        0x428a2f98u, 0x71374491u, 0xb5c0fbcfu, 0xe9b5dba5u, 0x3956c25bu, 0x59f111f1u,
+        0x923f82a4u, 0xab1c5ed5u, 0xd807aa98u, 0x12835b01u, 0x243185beu, 0x550c7dc3u,
+        0x72be5d74u, 0x80deb1feu, 0x9bdc06a7u, 0xc19bf174u, 0xe49b69c1u, 0xefbe4786u,
+        0x0fc19dc6u, 0x240ca1ccu, 0x2de92c6fu, 0x4a7484aau, 0x5cb0a9dcu, 0x76f988dau,
+        0x983e5152u, 0xa831c66du, 0xb00327c8u, 0xbf597fc7u, 0xc6e00bf3u, 0xd5a79147u,
+        0x06ca6351u, 0x14292967u, 0x27b70a85u, 0x2e1b2138u, 0x4d2c6dfcu, 0x53380d13u,
+        0x650a7354u, 0x766a0abbu, 0x81c2c92eu, 0x92722c85u, 0xa2bfe8a1u, 0xa81a664bu,
+        0xc24b8b70u, 0xc76c51a3u, 0xd192e819u, 0xd6990624u, 0xf40e3585u, 0x106aa070u,
+        0x19a4c116u, 0x1e376c08u, 0x2748774cu, 0x34b0bcb5u, 0x391c0cb3u, 0x4ed8aa4au,
+        0x5b9cca4fu, 0x682e6ff3u, 0x748f82eeu, 0x78a5636fu, 0x84c87814u, 0x8cc70208u,
+        0x90befffau, 0xa4506cebu, 0xbef9a3f7u, 0xc67178f2u};
+    uint32_t a = st[0], b = st[1], c = st[2], d = st[3];
+    uint32_t e = st[4], f = st[5], g = st[6], h = st[7];
+#pragma unroll
+    for (int t = 0; t < 64; t++) {
+        if (t >= 16) {
+            const uint32_t x15 = w[(t - 15) & 15], x2 = w[(t - 2) & 15];
+            const uint32_t s0 = ror32(x15, 7) ^ ror32(x15, 18) ^ (x15 >> 3);
+            const uint32_t s1 = ror32(x2, 17) ^ ror32(x2, 19) ^ (x2 >> 10);
+            w[t & 15] += s0 + w[(t - 7) & 15] + s1;
+        }
+        const uint32_t S1 = ror32(e, 6) ^ ror32(e, 11) ^ ror32(e, 25);
+        const uint32_t ch = g ^ (e & (f ^ g));
+        const uint32_t t1 = h + S1 + ch + K[t] + w[t & 15];
+        const uint32_t S0 = ror32(a, 2) ^ ror32(a, 13) ^ ror32(a, 22);
+        const uint32_t mj = (a & b) | (c & (a | b));
+        h = g; g = f; f = e; e = d + t1;
+        d = c; c = b; b = a; a = t1 + S0 + mj;
+    }
+    st[0] += a; st[1] += b; st[2] += c; st[3] += d;
+    st[4] += e; st[5] += f; st[6] += g; st[7] += h;
+}
+
+__device__ __forceinline__ void sha256_iv(uint32_t (&st)[8])
+{
+    st[0] = 0x6a09e667u; st[1] = 0xbb67ae85u; st[2] = 0x3c6ef372u; st[3] = 0xa54ff53au;
+    st[4] = 0x510e527fu; st[5] = 0x9b05688cu; st[6] = 0x1f83d9abu; st[7] = 0x5be0cd19u;
+}
+
+// SHA-256 of a message of MW big-endian words (4*MW bytes), from the IV.
+template <int MW>
+__device__ __forceinline__ void sha256_words(uint32_t (&out)[8], const uint32_t (&m)[MW])
+{
+    constexpr int NB = (MW * 4 + 9 + 63) / 64;
+    uint32_t st[8];
+    sha256_iv(st);
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        uint32_t w[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const int k = 16 * b + j;
+            w[j] = (k < MW) ? m[k < MW ? k : 0] : (k == MW ? 0x80000000u : 0u);
+        }
+        if (b == NB - 1) {
+            w[14] = 0;
+            w[15] = (uint32_t)(MW * 32);
+        }
+        sha256_compress(st, w);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) out[i] = st[i];
+}
+
+// ---------------------------------------------------------------------------
+// SHA-512 compression (FIPS 180-4 6.4.2).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t ror64(uint64_t x, int n) { return (x >> n) | (x << (64 - n)); }
+
+__device__ __forceinline__ void sha512_compress(uint64_t (&st)[8], uint64_t (&w)[16])
+{
+    const uint64_t K[80] = {
+        0x428a2f98d728ae22ull, 0x7137449123ef65cdull, 0xb5c0fbcfec4d3b2full, 0xe9b5dba58189dbbcull,
+        0x3956c25bf348b538ull, 0x59f111f1b605d019ull, 0x923f82a4af194f9bull, 0xab1c5ed5da6d8118ull,
+        0xd807aa98a3030242ull, 0x12835b0145706fbeull, 0x243185be4ee4b28cull, 0x550c7dc3d5ffb4e2ull,
+        0x72be5d74f27b896full, 0x80deb1fe3b1696b1ull, 0x9bdc06a725c71235ull, 0xc19bf174cf692694ull,
+        0xe49b69c19ef14ad2ull, 0xefbe4786384f25e3ull, 0x0fc19dc68b8cd5b5ull, 0x240ca1cc77ac9c65ull,
+        0x2de92c6f592b0275ull, 0x4a7484aa6ea6e483ull, 0x5cb0a9dcbd41fbd4ull, 0x76f988da831153b5ull,
+        0x983e5152ee66dfabull, 0xa831c66d2db43210ull, 0xb00327c898fb213full, 0xbf597fc7beef0ee4ull,
+        0xc6e00bf33da88fc2ull, 0xd5a79147930aa725ull, 0x06ca6351e003826full, 0x142929670a0e6e70ull,
+        0x27b70a8546d22ffcull, 0x2e1b21385c26c926ull, 0x4d2c6dfc5ac42aedull, 0x53380d139d95b3dfull,
+        0x650a73548baf63deull, 0x766a0abb3c77b2a8ull, 0x81c2c92e47edaee6ull, 0x92722c851482353bull,
+        0xa2bfe8a14cf10364ull, 0xa81a664bbc423001ull, 0xc24b8b70d0f89791ull, 0xc76c51a30654be30ull,
+        0xd192e819d6ef5218ull, 0xd69906245565a910ull, 0xf40e35855771202aull, 0x106aa07032bbd1b8ull,
+        0x19a4c116b8d2d0c8ull, 0x1e376c085141ab53ull, 0x2748774cdf8eeb99ull, 0x34b0bcb5e19b48a8ull,
+        0x391c0cb3c5c95a63ull, 0x4ed8aa4ae3418acbull, 0x5b9cca4f7763e373ull, 0x682e6ff3d6b2b8a3ull,
+        0x748f82ee5defb2fcull, 0x78a5636f43172f60ull, 0x84c87814a1f0ab72ull, 0x8cc702081a6439ecull,
+        0x90befffa23631e28ull, 0xa4506cebde82bde9ull, 0xbef9a3f7b2c67915ull, 0xc67178f2e372532bull,
+        0xca273eceea26619cull, 0xd186b8c721c0c207ull, 0xeada7dd6cde0eb1eull, 0xf57d4f7fee6ed178ull,
+        0x06f067aa72176fbaull, 0x0a637dc5a2c898a6ull, 0x113f9804bef90daeull, 0x1b710b35131c471bull,
+        0x28db77f523047d84ull, 0x32caab7b40c72493ull, 0x3c9ebe0a15c9bebcull, 0x431d67c49c100d4cull,
+        0x4cc5d4becb3e42b6ull, 0x597f299cfc657e2aull, 0x5fcb6fab3ad6faecull, 0x6c44198c4a475817ull};
+    uint64_t a = st[0], b = st[1], c = st[2], d = st[3];
+    uint64_t e = st[4], f = st[5], g = st[6], h = st[7];
+#pragma unroll
+    for (int t = 0; t < 80; t++) {
+        if (t >= 16) {
+            const uint64_t x15 = w[(t - 15) & 15], x2 = w[(t - 2) & 15];
+            const uint64_t s0 = ror64(x15, 1) ^ ror64(x15, 8) ^ (x15 >> 7);
+            const uint64_t s1 = ror64(x2, 19) ^ ror64(x2, 61) ^ (x2 >> 6);
+            w[t & 15] += s0 + w[(t - 7) & 15] + s1;
+        }
+        const uint64_t S1 = ror64(e, 14) ^ ror64(e, 18) ^ ror64(e, 41);
+        const uint64_t ch = g ^ (e & (f ^ g));
+        const uint64_t t1 = h + S1 + ch + K[t] + w[t & 15];
+        const uint64_t S0 = ror64(a, 28) ^ ror64(a, 34) ^ ror64(a, 39);
+        const uint64_t mj = (a & b) | (c & (a | b));
+        h = g; g = f; f = e; e = d + t1;
+        d = c; c = b; b = a; a = t1 + S0 + mj;
+    }
+    st[0] += a; st[1] += b; st[2] += c; st[3] += d;
+    st[4] += e; st[5] += f; st[6] += g; st[7] += h;
+}
+
+__device__ __forceinline__ void sha512_iv(uint64_t (&st)[8])
+{
+    st[0] = 0x6a09e667f3bcc908ull; st[1] = 0xbb67ae8584caa73bull;
+    st[2] = 0x3c6ef372fe94f82bull; st[3] = 0xa54ff53a5f1d36f1ull;
+    st[4] = 0x510e527fade682d1ull; st[5] = 0x9b05688c2b3e6c1full;
+    st[6] = 0x1f83d9abfb41bd6bull; st[7] = 0x5be0cd19137e2179ull;
+}
+
+__device__ __forceinline__ uint64_t join64(uint32_t hi, uint32_t lo)
+{
+    return ((uint64_t)hi << 32) | lo;
+}
+
+// SHA-512 of a message of MW big-endian 32-bit words (MW even), from the IV;
+// out holds 16 big-endian 32-bit words.
+template <int MW>
+__device__ __forceinline__ void sha512_words(uint32_t (&out)[16], const uint32_t (&m)[MW])
+{
+    static_assert(MW % 2 == 0, "SHA-512 messages here are whole 64-bit words");
+    constexpr int MQ = MW / 2;
+    constexpr int NB = (MW * 4 + 17 + 127) / 128;
+    uint64_t st[8];
+    sha512_iv(st);
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        uint64_t w[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const int k = 16 * b + j;
+            w[j] = (k < MQ) ? join64(m[2 * (k < MQ ? k : 0)], m[2 * (k < MQ ? k : 0) + 1])
+                            : (k == MQ ? 0x8000000000000000ull : 0ull);
+        }
+        if (b == NB - 1) {
+            w[14] = 0;
+            w[15] = (uint64_t)MW * 32;
+        }
+        sha512_compress(st, w);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        out[2 * i] = (uint32_t)(st[i] >> 32);
+        out[2 * i + 1] = (uint32_t)st[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Keccak-f[1600] (FIPS 202 3.2-3.3).  Lane A[x + 5y].
+// ---------------------------------------------------------------------------
+template <int N>
+__device__ __forceinline__ uint64_t rol64c(uint64_t x)
+{
+    if constexpr (N == 0) {
+        return x;
+    } else {
+        return (x << N) | (x >> (64 - N));
+    }
+}
+
+// rho offsets r[x + 5y] (FIPS 202 Algorithm 2)
+template <int I>
+struct KeccakRho {
+    static constexpr int tbl[25] = {0,  1,  62, 28, 27, 36, 44, 6,  55, 20, 3,  10, 43,
+                                    25, 39, 41, 45, 15, 21, 8,  18, 2,  61, 56, 14};
+    static constexpr int value = tbl[I];
+};
+
+template <int I>
+__device__ __forceinline__ void keccak_rho_pi(uint64_t (&B)[25], const uint64_t (&A)[25],
+                                              const uint64_t (&D)[5])
+{
+    constexpr int x = I % 5, y = I / 5;
+    constexpr int dst = y + 5 * ((2 * x + 3 * y) % 5);
+    B[dst] = rol64c<KeccakRho<I>::value>(A[I] ^ D[x]);
+    if constexpr (I + 1 < 25) keccak_rho_pi<I + 1>(B, A, D);
+}
+
+__device__ __forceinline__ void keccak_f1600(uint64_t (&A)[25])
+{
+    const uint64_t RC[24] = {
+        0x0000000000000001ull, 0x0000000000008082ull, 0x800000000000808aull, 0x8000000080008000ull,
+        0x000000000000808bull, 0x0000000080000001ull, 0x8000000080008081ull, 0x8000000000008009ull,
+        0x000000000000008aull, 0x0000000000000088ull, 0x0000000080008009ull, 0x000000008000000aull,
+        0x000000008000808bull, 0x800000000000008bull, 0x8000000000008089ull, 0x8000000000008003ull,
+        0x8000000000008002ull, 0x8000000000000080ull, 0x000000000000800aull, 0x800000008000000aull,
+        0x8000000080008081ull, 0x8000000000008080ull, 0x0000000080000001ull, 0x8000000080008008ull};
+#pragma unroll
+    for (int r = 0; r < 24; r++) {
+        uint64_t C[5], D[5], B[25];
+#pragma unroll
+        for (int x = 0; x < 5; x++) C[x] = A[x] ^ A[x + 5] ^ A[x + 10] ^ A[x + 15] ^ A[x + 20];
+#pragma unroll
+        for (int x = 0; x < 5; x++) D[x] = C[(x + 4) % 5] ^ rol64c<1>(C[(x + 1) % 5]);
+        keccak_rho_pi<0>(B, A, D);
+#pragma unroll
+        for (int y = 0; y < 5; y++) {
+#pragma unroll
+            for (int x = 0; x < 5; x++) {
+                A[x + 5 * y] = B[x + 5 * y] ^ (~B[(x + 1) % 5 + 5 * y] & B[(x + 2) % 5 + 5 * y]);
+            }
+        }
+        A[0] ^= RC[r];
+    }
+}
+
+// SHAKE with rate RATEW 32-bit words (42 = SHAKE128, 34 = SHAKE256) over a
+// message of MW little-endian words; writes the first OUTW output words.
+template <int RATEW, int MW, int OUTW>
+__device__ __forceinline__ void shake_words(uint32_t (&out)[OUTW], const uint32_t (&m)[MW])
+{
+    static_assert(OUTW <= RATEW, "output fits in one squeeze block");
+    constexpr int NB = (MW * 4) / (RATEW * 4) + 1;  // absorbed blocks incl. padding
+    uint64_t A[25];
+#pragma unroll
+    for (int i = 0; i < 25; i++) A[i] = 0;
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+#pragma unroll
+        for (int i = 0; i < RATEW / 2; i++) {
+            uint32_t lo = 0, hi = 0;
+            const int k0 = b * RATEW + 2 * i, k1 = k0 + 1;
+            if (k0 < MW) lo = m[k0 < MW ? k0 : 0];
+            else if (k0 == MW) lo = 0x1Fu;
+            if (k1 < MW) hi = m[k1 < MW ? k1 : 0];
+            else if (k1 == MW) hi = 0x1Fu;
+            if (b == NB - 1 && 2 * i + 1 == RATEW - 1) hi ^= 0x80000000u;
+            A[i] ^= ((uint64_t)hi << 32) | lo;
+        }
+        keccak_f1600(A);
+    }
+#pragma unroll
+    for (int i = 0; i < OUTW; i++) out[i] = (i & 1) ? (uint32_t)(A[i / 2] >> 32) : (uint32_t)A[i / 2];
+}
+
+}  // namespace xb

@@ -1,0 +1,60 @@
+// Compression-rate probe: every thread runs `iters` dependent SHA-256
+// compressions (or Keccak-f[1600] permutations) entirely in registers.  It
+// measures the chip's sustained rate for the same compression code the XMSS
+// kernels use and is the denominator of their roofline fraction.
+#include <cstdint>
+
+#include "engine.h"
+#include "hashcore.cuh"
+
+namespace xb {
+
+__global__ void __launch_bounds__(128) k_sha256_rate(uint32_t iters, uint32_t seed, uint32_t* __restrict__ sink)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t st[8];
+    sha256_iv(st);
+    st[0] ^= t;
+    st[1] ^= seed;
+#pragma unroll 1
+    for (uint32_t i = 0; i < iters; i++) {
+        uint32_t w[16];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            w[j] = st[j];
+            w[8 + j] = st[j] ^ i;
+        }
+        sha256_compress(st, w);
+    }
+    uint32_t x = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) x ^= st[j];
+    if (x == 0x9E3779B9u) sink[t] = x;  // practically never; keeps the work live
+}
+
+__global__ void __launch_bounds__(128) k_keccak_rate(uint32_t iters, uint32_t seed, uint32_t* __restrict__ sink)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t A[25];
+#pragma unroll
+    for (int j = 0; j < 25; j++) A[j] = ((uint64_t)t << 32) ^ seed ^ j;
+#pragma unroll 1
+    for (uint32_t i = 0; i < iters; i++) {
+        A[0] ^= i;
+        keccak_f1600(A);
+    }
+    uint64_t x = 0;
+#pragma unroll
+    for (int j = 0; j < 25; j++) x ^= A[j];
+    if ((uint32_t)x == 0x9E3779B9u) sink[t] = (uint32_t)x;
+}
+
+void launch_rate(int kind, uint32_t blocks, uint32_t iters, uint32_t* sink, cudaStream_t st)
+{
+    if (kind == 0)
+        k_sha256_rate<<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink);
+    else
+        k_keccak_rate<<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink);
+}
+
+}  // namespace xb

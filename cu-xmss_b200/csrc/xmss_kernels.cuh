@@ -1,0 +1,543 @@
+// XMSS / XMSS^MT kernels for sm_100a, templated over a hash family F
+// (families.cuh).  The hot path is split into phases with flat work lists so
+// every launch has one uniform work item per thread:
+//
+//   keygen / tree build   chains (PRF_keygen + 15 F per chain)
+//                         -> L-tree levels -> Merkle tree levels
+//   verify                prep (H_msg + base_w) -> chains (len_i .. 14)
+//                         -> L-tree levels -> root (compute_root, compare)
+//   sign                  trees (as keygen) -> prep (R, H_msg, auth paths,
+//                         base_w of every layer) -> chains (0 .. len_i - 1)
+//
+// Reference functions restated here (cuxmss/): wots.c:14-175 (expand_seed,
+// gen_chain, base_w, checksum), xmss_commons.c:16-96 (l_tree, compute_root),
+// xmss_core.c:19-86 (treehash as level-synchronous reduction),
+// xmss_commons.c:136-215 (sign_open), xmss_core.c:183-273 (sign).
+#pragma once
+
+#include <cstdint>
+
+#include "families.cuh"
+
+namespace xb {
+
+enum : uint32_t { ADDR_OTS = 0, ADDR_LTREE = 1, ADDR_HASHTREE = 2 };
+
+// One WOTS leaf slot of an L-tree launch: its address and where the leaf goes.
+struct LeafRef {
+    uint32_t key;
+    uint32_t layer;
+    uint64_t tree;
+    uint32_t leaf;
+    uint32_t pad;
+    uint64_t out_off;  // byte offset of the finished leaf in the leaf output
+};
+
+// One Merkle subtree to build (all jobs of a launch share the same height).
+struct TreeJob {
+    uint32_t key;
+    uint32_t layer;
+    uint64_t tree;
+    uint64_t node_off;  // byte offset of the node array (levels 0..h, level-major)
+};
+
+// Byte offset (in nodes) of level l inside a subtree node array of height h.
+__host__ __device__ __forceinline__ uint64_t level_offset(int h, int l)
+{
+    return (2ull << h) - (2ull << (h - l));
+}
+
+__device__ __forceinline__ void set_addr(uint32_t (&a)[8], uint32_t layer, uint64_t tree, uint32_t type,
+                                         uint32_t w4, uint32_t w5, uint32_t w6)
+{
+    a[0] = layer;
+    a[1] = (uint32_t)(tree >> 32);
+    a[2] = (uint32_t)tree;
+    a[3] = type;
+    a[4] = w4;
+    a[5] = w5;
+    a[6] = w6;
+    a[7] = 0;
+}
+
+__device__ __forceinline__ uint64_t bytes_be(const uint8_t* p, int len)
+{
+    uint64_t r = 0;
+    for (int i = 0; i < len; i++) r = (r << 8) | p[i];
+    return r;
+}
+
+// base_w of the n-byte message plus the checksum digits (wots.c:60-107);
+// writes the LEN chain start positions.
+template <class F>
+__device__ __forceinline__ void chain_lengths(uint8_t* lens, const uint32_t (&msg)[F::NW])
+{
+    int csum = 0;
+#pragma unroll
+    for (int k = 0; k < F::N; k++) {
+        const uint32_t b = F::byte_at(msg, k);
+        lens[2 * k] = (uint8_t)(b >> 4);
+        lens[2 * k + 1] = (uint8_t)(b & 15);
+        csum += 30 - (int)(b >> 4) - (int)(b & 15);
+    }
+    // len2 = 3 digits of csum << 4, i.e. the top 12 bits of a 16-bit value
+    csum <<= 4;
+    lens[F::LEN1] = (uint8_t)((csum >> 12) & 15);
+    lens[F::LEN1 + 1] = (uint8_t)((csum >> 8) & 15);
+    lens[F::LEN1 + 2] = (uint8_t)((csum >> 4) & 15);
+}
+
+// Per-key contexts from strided rows of PUB_SEED, SK_SEED and SK_PRF (the
+// secret rows may be absent for verify-only keys).
+template <class F>
+__global__ void k_make_ctx(const uint8_t* __restrict__ pub, uint32_t pub_stride, const uint8_t* __restrict__ sks,
+                           uint32_t sks_stride, const uint8_t* __restrict__ skp, uint32_t skp_stride,
+                           uint32_t nkeys, typename F::Ctx* __restrict__ ctx)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nkeys) return;
+    typename F::Ctx c;
+    F::make_ctx(c, pub + (size_t)k * pub_stride, sks ? sks + (size_t)k * sks_stride : nullptr,
+                skp ? skp + (size_t)k * skp_stride : nullptr);
+    ctx[k] = c;
+}
+
+// ---------------------------------------------------------------------------
+// Tree building.
+// ---------------------------------------------------------------------------
+
+// One thread per (job, leaf, chain): PRF_keygen then the full chain (15 F),
+// i.e. expand_seed + gen_chain(0, w-1) of wots_pkgen (wots.c:117-131).
+// Leaf slots are numbered job-major (slot = job << h | leaf); one launch
+// covers slots [slot0, slot0 + nslots) and indexes wpk / refs from slot0.
+template <class F>
+__global__ void __launch_bounds__(128) k_keygen_chains(const TreeJob* __restrict__ jobs, int h, uint64_t slot0,
+                                                       uint64_t nslots, const typename F::Ctx* __restrict__ ctx,
+                                                       uint8_t* __restrict__ wpk, LeafRef* __restrict__ refs)
+{
+    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= nslots * F::LEN) return;
+    const uint64_t local = item / F::LEN;
+    const uint32_t chain = (uint32_t)(item - local * F::LEN);
+    const uint64_t slot = slot0 + local;
+    const uint32_t j = (uint32_t)(slot >> h);
+    const uint32_t leaf = (uint32_t)(slot & ((1ull << h) - 1));
+    const TreeJob job = jobs[j];
+    const typename F::Ctx& c = ctx[job.key];
+    uint32_t a[8], x[F::NW];
+    set_addr(a, job.layer, job.tree, ADDR_OTS, leaf, chain, 0);
+    F::prf_keygen(x, c, a);
+#pragma unroll 1
+    for (uint32_t i = 0; i < 15; i++) {
+        a[6] = i;
+        F::thash_f(x, c, a);
+    }
+    F::store(wpk + item * F::N, x);
+    if (chain == 0) {
+        LeafRef r;
+        r.key = job.key;
+        r.layer = job.layer;
+        r.tree = job.tree;
+        r.leaf = leaf;
+        r.pad = 0;
+        r.out_off = job.node_off + (uint64_t)leaf * F::N;
+        refs[local] = r;
+    }
+}
+
+// One L-tree level (xmss_commons.c:16-49) for many leaf slots: item =
+// (slot, pair).  Pairs hash nodes 2p, 2p+1; an odd last node is carried up.
+// The final level (cnt_in == 2) writes the leaf to leaf_out + ref.out_off.
+template <class F>
+__global__ void __launch_bounds__(128) k_ltree_level(const LeafRef* __restrict__ refs, uint32_t nslots, int level,
+                                                     int cnt_in, const uint8_t* __restrict__ src, uint32_t src_stride,
+                                                     uint8_t* __restrict__ dst, uint32_t dst_stride,
+                                                     uint8_t* __restrict__ leaf_out,
+                                                     const typename F::Ctx* __restrict__ ctx,
+                                                     const int* __restrict__ status)
+{
+    const int pairs = (cnt_in + 1) >> 1;
+    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= (uint64_t)nslots * pairs) return;
+    const uint32_t slot = (uint32_t)(item / pairs);
+    const int p = (int)(item - (uint64_t)slot * pairs);
+    if (status && status[slot] != 0) return;
+    const LeafRef r = refs[slot];
+    const uint8_t* s = src + ((uint64_t)slot * src_stride) * F::N;
+    uint8_t* out = (cnt_in == 2) ? leaf_out + r.out_off : dst + ((uint64_t)slot * dst_stride + p) * F::N;
+    uint32_t l[F::NW], rr[F::NW], o[F::NW];
+    F::load(l, s + (uint64_t)(2 * p) * F::N);
+    if (2 * p + 1 < cnt_in) {
+        F::load(rr, s + (uint64_t)(2 * p + 1) * F::N);
+        uint32_t a[8];
+        set_addr(a, r.layer, r.tree, ADDR_LTREE, r.leaf, (uint32_t)level, (uint32_t)p);
+        F::thash_h(o, l, rr, ctx[r.key], a);
+        F::store(out, o);
+    } else {
+        F::store(out, l);
+    }
+}
+
+// One Merkle level of many subtrees of equal height h: item = (job, node i
+// of level+1) = H(child 2i, child 2i+1) with tree_height = level, tree_index
+// = i (xmss_core.c:62-83).
+template <class F>
+__global__ void __launch_bounds__(128) k_tree_level(const TreeJob* __restrict__ jobs, uint32_t njobs, int h, int level,
+                                                    uint8_t* __restrict__ nodes,
+                                                    const typename F::Ctx* __restrict__ ctx)
+{
+    const int sh = h - level - 1;
+    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= ((uint64_t)njobs << sh)) return;
+    const uint32_t j = (uint32_t)(item >> sh);
+    const uint32_t i = (uint32_t)(item & ((1ull << sh) - 1));
+    const TreeJob job = jobs[j];
+    uint8_t* base = nodes + job.node_off;
+    uint32_t l[F::NW], r[F::NW], o[F::NW], a[8];
+    F::load(l, base + (level_offset(h, level) + 2ull * i) * F::N);
+    F::load(r, base + (level_offset(h, level) + 2ull * i + 1) * F::N);
+    set_addr(a, job.layer, job.tree, ADDR_HASHTREE, 0, (uint32_t)level, i);
+    F::thash_h(o, l, r, ctx[job.key], a);
+    F::store(base + (level_offset(h, level + 1) + i) * F::N, o);
+}
+
+// ---------------------------------------------------------------------------
+// Verify (xmss_commons.c:136-215).
+// ---------------------------------------------------------------------------
+struct VerifyArgs {
+    const uint8_t* sm;        // concatenated signed messages
+    const uint64_t* sm_off;   // [count] byte offset of each sm
+    const uint64_t* smlen;    // [count]
+    const uint32_t* key;      // [count] key index
+    const uint8_t* key_root;  // public root of key k at key_root + k * key_stride
+    uint32_t key_stride;
+    uint8_t* node;            // [count][N] running message / root
+    uint8_t* lens;            // [count][LEN] chain start positions
+    uint64_t* idx;            // [count]
+    int* status;              // [count] 0 = valid so far
+    uint8_t* wpk;             // [count][LEN][N]
+    uint8_t* wpk2;            // [count][LEN/2 + 1][N]
+    uint8_t* leaf;            // [count][N]
+    LeafRef* refs;            // [count]
+    unsigned long long* work;  // [3] H_msg blocks, F calls, H calls (accumulated)
+    uint32_t count;
+    uint32_t index_bytes;
+    uint32_t sig_bytes;
+    uint32_t tree_height;
+    uint32_t d;
+};
+
+// Hash blocks H_msg absorbs for a message of mlen bytes (prefix pl + 3n).
+template <class F>
+__device__ __forceinline__ unsigned long long hmsg_blocks(uint64_t mlen)
+{
+    const uint64_t L = (uint64_t)F::PL + 3 * F::N + mlen;
+    constexpr int K = HMsgKind<F>::v;
+    if constexpr (K == 0) return (L + 9 + 63) / 64;
+    else if constexpr (K == 1) return (L + 17 + 127) / 128;
+    else return L / (4 * K) + 1;
+}
+
+template <class F>
+__device__ __forceinline__ unsigned long long chain_steps(const uint8_t* lens)
+{
+    unsigned long long s = 0;
+    for (int i = 0; i < F::LEN; i++) s += 15 - lens[i];
+    return s;
+}
+
+template <class F>
+__global__ void k_verify_prep(VerifyArgs v, const typename F::Ctx* __restrict__ ctx)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.count) return;
+    const uint64_t smlen = v.smlen[s];
+    if (smlen < v.sig_bytes) {  // the reference would underflow here; reject
+        v.status[s] = -1;
+        return;
+    }
+    const uint8_t* sm = v.sm + v.sm_off[s];
+    const uint64_t idx = bytes_be(sm, (int)v.index_bytes);
+    uint32_t R[F::NW], root[F::NW], mh[F::NW];
+    F::load(R, sm + v.index_bytes);
+    F::load(root, v.key_root + (uint64_t)v.key[s] * v.key_stride);
+    hmsg<F>(mh, R, root, idx, sm + v.sig_bytes, smlen - v.sig_bytes);
+    F::store(v.node + (uint64_t)s * F::N, mh);
+    uint8_t* lens = v.lens + (uint64_t)s * F::LEN;
+    chain_lengths<F>(lens, mh);
+    v.idx[s] = idx;
+    v.status[s] = 0;
+    if (v.work) {
+        atomicAdd(&v.work[0], hmsg_blocks<F>(smlen - v.sig_bytes));
+        atomicAdd(&v.work[1], chain_steps<F>(lens));
+        atomicAdd(&v.work[2], (unsigned long long)(F::LEN - 1 + v.tree_height) * v.d);
+    }
+}
+
+// One thread per (signature, chain): gen_chain(len_i, w-1-len_i) of
+// wots_pk_from_sig (wots.c:161-175).
+template <class F>
+__global__ void __launch_bounds__(128) k_verify_chains(VerifyArgs v, uint32_t layer,
+                                                       const typename F::Ctx* __restrict__ ctx)
+{
+    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= (uint64_t)v.count * F::LEN) return;
+    const uint32_t s = (uint32_t)(item / F::LEN);
+    const uint32_t chain = (uint32_t)(item - (uint64_t)s * F::LEN);
+    if (v.status[s] != 0) return;
+    const uint64_t idx = v.idx[s];
+    const uint32_t th = v.tree_height;
+    const uint32_t leaf = (uint32_t)((idx >> (th * layer)) & ((1ull << th) - 1));
+    const uint64_t tree = (th * (layer + 1) >= 64) ? 0 : idx >> (th * (layer + 1));
+    const uint32_t start = v.lens[(uint64_t)s * F::LEN + chain];
+    const uint64_t wsb = (uint64_t)F::LEN * F::N;
+    const uint8_t* sig = v.sm + v.sm_off[s] + v.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N);
+    uint32_t x[F::NW], a[8];
+    F::load(x, sig + (uint64_t)chain * F::N);
+    set_addr(a, layer, tree, ADDR_OTS, leaf, chain, 0);
+    const typename F::Ctx& c = ctx[v.key[s]];
+#pragma unroll 1
+    for (uint32_t i = start; i < 15; i++) {
+        a[6] = i;
+        F::thash_f(x, c, a);
+    }
+    F::store(v.wpk + item * F::N, x);
+    if (chain == 0) {
+        LeafRef r;
+        r.key = v.key[s];
+        r.layer = layer;
+        r.tree = tree;
+        r.leaf = leaf;
+        r.pad = 0;
+        r.out_off = (uint64_t)s * F::N;
+        v.refs[s] = r;
+    }
+}
+
+// compute_root (xmss_commons.c:54-96) for one layer; then either the next
+// layer's chain lengths or the final comparison with the public root.
+template <class F>
+__global__ void k_verify_root(VerifyArgs v, uint32_t layer, const typename F::Ctx* __restrict__ ctx)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.count || v.status[s] != 0) return;
+    const uint64_t idx = v.idx[s];
+    const uint32_t th = v.tree_height;
+    uint32_t leafidx = (uint32_t)((idx >> (th * layer)) & ((1ull << th) - 1));
+    const uint64_t tree = (th * (layer + 1) >= 64) ? 0 : idx >> (th * (layer + 1));
+    const uint64_t wsb = (uint64_t)F::LEN * F::N;
+    const uint8_t* auth =
+        v.sm + v.sm_off[s] + v.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N) + wsb;
+    const typename F::Ctx& c = ctx[v.key[s]];
+    uint32_t cur[F::NW], sib[F::NW], a[8];
+    F::load(cur, v.leaf + (uint64_t)s * F::N);
+#pragma unroll 1
+    for (uint32_t i = 0; i < th; i++) {
+        F::load(sib, auth + (uint64_t)i * F::N);
+        const uint32_t odd = leafidx & 1;
+        leafidx >>= 1;
+        set_addr(a, layer, tree, ADDR_HASHTREE, 0, i, leafidx);
+        if (odd) {
+            F::thash_h(cur, sib, cur, c, a);
+        } else {
+            F::thash_h(cur, cur, sib, c, a);
+        }
+    }
+    if (layer + 1 < v.d) {
+        F::store(v.node + (uint64_t)s * F::N, cur);
+        uint8_t* lens = v.lens + (uint64_t)s * F::LEN;
+        chain_lengths<F>(lens, cur);
+        if (v.work) atomicAdd(&v.work[1], chain_steps<F>(lens));
+    } else {
+        uint32_t pr[F::NW];
+        F::load(pr, v.key_root + (uint64_t)v.key[s] * v.key_stride);
+        uint32_t diff = 0;
+#pragma unroll
+        for (int i = 0; i < F::NW; i++) diff |= pr[i] ^ cur[i];
+        v.status[s] = diff ? -1 : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Sign (xmss_core.c:183-273) given built subtrees.
+// ---------------------------------------------------------------------------
+struct SignArgs {
+    uint8_t* sm;              // concatenated output buffers; M already at sm + sig_bytes
+    const uint64_t* sm_off;   // [count]
+    const uint64_t* mlen;     // [count]
+    const uint64_t* idx;      // [count] one-time index of each signature
+    const uint32_t* key;      // [count]
+    const uint8_t* key_root;  // public root of key k at key_root + k * key_stride
+    uint32_t key_stride;
+    const uint64_t* tree_off; // [count][d] byte offset of each layer's subtree node array
+    const uint8_t* nodes;     // subtree node arrays
+    uint8_t* lens;            // [count][d][LEN]
+    uint32_t count;
+    uint32_t index_bytes;
+    uint32_t sig_bytes;
+    uint32_t tree_height;
+    uint32_t d;
+};
+
+// One thread per signature: R, H_msg, every layer's chain lengths (layer 0
+// signs the message digest, layer i signs the root of layer i-1) and the
+// authentication paths copied out of the subtree node arrays.
+template <class F>
+__global__ void k_sign_prep(SignArgs g, const typename F::Ctx* __restrict__ ctx)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.count) return;
+    uint8_t* sm = g.sm + g.sm_off[s];
+    const uint64_t idx = g.idx[s];
+    const typename F::Ctx& c = ctx[g.key[s]];
+    const uint32_t th = g.tree_height;
+    uint32_t R[F::NW], root[F::NW], mh[F::NW];
+    F::prf_r(R, c, idx);
+    F::store(sm + g.index_bytes, R);
+    F::load(root, g.key_root + (uint64_t)g.key[s] * g.key_stride);
+    hmsg<F>(mh, R, root, idx, sm + g.sig_bytes, g.mlen[s]);
+    const uint64_t wsb = (uint64_t)F::LEN * F::N;
+    for (uint32_t layer = 0; layer < g.d; layer++) {
+        const uint8_t* tn = g.nodes + g.tree_off[(uint64_t)s * g.d + layer];
+        const uint32_t leaf = (uint32_t)((idx >> (th * layer)) & ((1ull << th) - 1));
+        if (layer == 0) {
+            chain_lengths<F>(g.lens + ((uint64_t)s * g.d) * F::LEN, mh);
+        } else {
+            uint32_t r[F::NW];
+            const uint8_t* prev = g.nodes + g.tree_off[(uint64_t)s * g.d + layer - 1];
+            F::load(r, prev + level_offset((int)th, (int)th) * F::N);
+            chain_lengths<F>(g.lens + ((uint64_t)s * g.d + layer) * F::LEN, r);
+        }
+        uint8_t* auth = sm + g.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N) + wsb;
+        for (uint32_t l = 0; l < th; l++) {
+            uint32_t v[F::NW];
+            F::load(v, tn + (level_offset((int)th, (int)l) + ((leaf >> l) ^ 1)) * F::N);
+            F::store(auth + (uint64_t)l * F::N, v);
+        }
+    }
+}
+
+// One thread per (signature, layer, chain): PRF_keygen then gen_chain(0,
+// len_i) of wots_sign (wots.c:136-154).
+template <class F>
+__global__ void __launch_bounds__(128) k_sign_chains(SignArgs g, const typename F::Ctx* __restrict__ ctx)
+{
+    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= (uint64_t)g.count * g.d * F::LEN) return;
+    const uint64_t sl = item / F::LEN;
+    const uint32_t chain = (uint32_t)(item - sl * F::LEN);
+    const uint32_t s = (uint32_t)(sl / g.d);
+    const uint32_t layer = (uint32_t)(sl - (uint64_t)s * g.d);
+    const uint64_t idx = g.idx[s];
+    const uint32_t th = g.tree_height;
+    const uint32_t leaf = (uint32_t)((idx >> (th * layer)) & ((1ull << th) - 1));
+    const uint64_t tree = (th * (layer + 1) >= 64) ? 0 : idx >> (th * (layer + 1));
+    const uint32_t steps = g.lens[item];
+    const typename F::Ctx& c = ctx[g.key[s]];
+    uint32_t x[F::NW], a[8];
+    set_addr(a, layer, tree, ADDR_OTS, leaf, chain, 0);
+    F::prf_keygen(x, c, a);
+#pragma unroll 1
+    for (uint32_t i = 0; i < steps; i++) {
+        a[6] = i;
+        F::thash_f(x, c, a);
+    }
+    const uint64_t wsb = (uint64_t)F::LEN * F::N;
+    uint8_t* sig = g.sm + g.sm_off[s] + g.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N);
+    F::store(sig + (uint64_t)chain * F::N, x);
+}
+
+// ---------------------------------------------------------------------------
+// Batched core_hash (hash.c:29-65) with a WOTS-style single-message stream:
+// digest of M under the family's hash (SHA-256 [truncated], SHA-512,
+// SHAKE128/256 with n output bytes).  Used to check the hash cores.
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void k_core_hash(const uint8_t* __restrict__ msgs, const uint64_t* __restrict__ off,
+                            const uint64_t* __restrict__ len, uint32_t count, uint8_t* __restrict__ out)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    const uint8_t* m = msgs + off[s];
+    const uint64_t L = len[s];
+    uint32_t o[F::NW];
+    constexpr int K = HMsgKind<F>::v;
+    if constexpr (K == 0) {
+        const uint64_t nb = (L + 9 + 63) / 64;
+        uint32_t st[8];
+        sha256_iv(st);
+        for (uint64_t b = 0; b < nb; b++) {
+            uint32_t w[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                const uint64_t p = 64 * b + 4 * j;
+                uint32_t le = (p < L) ? fetch4_le(m, L, p) : 0;
+                if (p <= L && L < p + 4) le |= 0x80u << (8 * (L - p));
+                w[j] = bswap32(le);
+            }
+            if (b == nb - 1) {
+                w[14] = (uint32_t)((L * 8) >> 32);
+                w[15] = (uint32_t)(L * 8);
+            }
+            sha256_compress(st, w);
+        }
+#pragma unroll
+        for (int i = 0; i < F::NW; i++) o[i] = st[i];
+    } else if constexpr (K == 1) {
+        const uint64_t nb = (L + 17 + 127) / 128;
+        uint64_t st[8];
+        sha512_iv(st);
+        for (uint64_t b = 0; b < nb; b++) {
+            uint64_t w[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                uint32_t hl[2];
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    const uint64_t p = 128 * b + 8 * j + 4 * q;
+                    uint32_t le = (p < L) ? fetch4_le(m, L, p) : 0;
+                    if (p <= L && L < p + 4) le |= 0x80u << (8 * (L - p));
+                    hl[q] = bswap32(le);
+                }
+                w[j] = join64(hl[0], hl[1]);
+            }
+            if (b == nb - 1) {
+                w[14] = 0;
+                w[15] = L * 8;
+            }
+            sha512_compress(st, w);
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            if (2 * i < F::NW) o[2 * i] = (uint32_t)(st[i] >> 32);
+            if (2 * i + 1 < F::NW) o[2 * i + 1] = (uint32_t)st[i];
+        }
+    } else {
+        const uint64_t RB = 4 * K;
+        const uint64_t nb = L / RB + 1;
+        uint64_t A[25];
+#pragma unroll
+        for (int i = 0; i < 25; i++) A[i] = 0;
+        for (uint64_t b = 0; b < nb; b++) {
+#pragma unroll
+            for (int i = 0; i < K / 2; i++) {
+                uint32_t hl[2];
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    const uint64_t p = RB * b + 8 * i + 4 * q;
+                    uint32_t le = (p < L) ? fetch4_le(m, L, p) : 0;
+                    if (p <= L && L < p + 4) le ^= 0x1Fu << (8 * (L - p));
+                    hl[q] = le;
+                }
+                if (b == nb - 1 && 2 * i + 1 == K - 1) hl[1] ^= 0x80000000u;
+                A[i] ^= ((uint64_t)hl[1] << 32) | hl[0];
+            }
+            keccak_f1600(A);
+        }
+#pragma unroll
+        for (int i = 0; i < F::NW; i++) o[i] = (i & 1) ? (uint32_t)(A[i / 2] >> 32) : (uint32_t)A[i / 2];
+    }
+    F::store(out + (uint64_t)s * F::N, o);
+}
+
+}  // namespace xb

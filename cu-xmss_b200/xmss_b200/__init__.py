@@ -1,0 +1,402 @@
+"""Python bindings of libxmss_b200.so, the sm_100a XMSS / XMSS^MT library.
+
+The functions mirror the reference's C API (cuxmss/xmss.h, xmss_core.h,
+params.h) with Python return values instead of output pointers:
+
+    xmss_keypair(oid)                 -> (ret, pk, sk)
+    xmss_sign(sk, m)                  -> (ret, sk_updated, sm)
+    xmss_sign_open(sm, pk)            -> (ret, m)
+    xmssmt_* likewise; xmssmt_core_seed_keypair(params, seed) -> (ret, pk, sk)
+
+plus the batch / device entry points of include/xmss_b200.h.  Every call
+runs on the GPU; importing this module fails loudly when the shared library
+has not been built (python -c "import __graft_entry__ as g; g.build()").
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from typing import Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libxmss_b200.so")
+INCLUDE_DIR = os.path.join(os.path.dirname(os.path.dirname(HERE)), "include")
+
+XMSS_SHA2, XMSS_SHAKE128, XMSS_SHAKE256 = 0, 1, 2
+XMSS_OID_LEN = 4
+GPU_FAILURE = -3
+
+
+class XmssParams(C.Structure):
+    """xmss_params (include/params.h; cuxmss/params.h:15-33)."""
+
+    _fields_ = [
+        ("func", C.c_uint), ("n", C.c_uint), ("padding_len", C.c_uint), ("wots_w", C.c_uint),
+        ("wots_log_w", C.c_uint), ("wots_len1", C.c_uint), ("wots_len2", C.c_uint),
+        ("wots_len", C.c_uint), ("wots_sig_bytes", C.c_uint), ("full_height", C.c_uint),
+        ("tree_height", C.c_uint), ("d", C.c_uint), ("index_bytes", C.c_uint),
+        ("sig_bytes", C.c_uint), ("pk_bytes", C.c_uint), ("sk_bytes", C.c_ulonglong),
+        ("bds_k", C.c_uint),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Work(C.Structure):
+    _fields_ = [("hmsg_blocks", C.c_ulonglong), ("f_calls", C.c_ulonglong), ("h_calls", C.c_ulonglong)]
+
+
+class GpuError(RuntimeError):
+    pass
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C cu-xmss_b200` "
+                          "(or __graft_entry__.build()); there is no CPU fallback")
+    return C.CDLL(LIB_PATH, mode=os.RTLD_LOCAL | os.RTLD_NOW)
+
+
+lib = _load()
+_u8p = C.POINTER(C.c_uint8)
+_u64p = C.POINTER(C.c_uint64)
+_ullp = C.POINTER(C.c_ulonglong)
+_u32p = C.POINTER(C.c_uint32)
+_intp = C.POINTER(C.c_int)
+
+lib.xmss_str_to_oid.argtypes = [_u32p, C.c_char_p]
+lib.xmssmt_str_to_oid.argtypes = [_u32p, C.c_char_p]
+lib.xmss_parse_oid.argtypes = [C.POINTER(XmssParams), C.c_uint32]
+lib.xmssmt_parse_oid.argtypes = [C.POINTER(XmssParams), C.c_uint32]
+lib.xmss_xmssmt_initialize_params.argtypes = [C.POINTER(XmssParams)]
+lib.xmss_xmssmt_core_sk_bytes.argtypes = [C.POINTER(XmssParams)]
+lib.xmss_xmssmt_core_sk_bytes.restype = C.c_ulonglong
+for _f in ("xmss_keypair", "xmssmt_keypair"):
+    getattr(lib, _f).argtypes = [_u8p, _u8p, C.c_uint32]
+for _f in ("xmss_sign", "xmssmt_sign"):
+    getattr(lib, _f).argtypes = [_u8p, _u8p, _ullp, _u8p, C.c_ulonglong]
+for _f in ("xmss_sign_open", "xmssmt_sign_open"):
+    getattr(lib, _f).argtypes = [_u8p, _ullp, _u8p, C.c_ulonglong, _u8p]
+lib.xmssmt_core_seed_keypair.argtypes = [C.POINTER(XmssParams), _u8p, _u8p, _u8p]
+for _f in ("xmss_core_keypair", "xmssmt_core_keypair"):
+    getattr(lib, _f).argtypes = [C.POINTER(XmssParams), _u8p, _u8p]
+for _f in ("xmss_core_sign", "xmssmt_core_sign"):
+    getattr(lib, _f).argtypes = [C.POINTER(XmssParams), _u8p, _u8p, _ullp, _u8p, C.c_ulonglong]
+for _f in ("xmss_core_sign_open", "xmssmt_core_sign_open"):
+    getattr(lib, _f).argtypes = [C.POINTER(XmssParams), _u8p, _ullp, _u8p, C.c_ulonglong, _u8p]
+lib.xmss_b200_init.argtypes = [C.c_int]
+lib.xmss_b200_last_error.restype = C.c_char_p
+_RNG = C.CFUNCTYPE(None, _u8p, C.c_ulonglong)
+lib.xmss_b200_set_randombytes.argtypes = [_RNG]
+lib.xmss_b200_supported.argtypes = [C.c_uint, C.c_uint]
+lib.xmss_b200_keypair_batch.argtypes = [C.c_uint32, C.c_int, C.c_uint32, _u8p, _u8p, _u8p]
+lib.xmss_b200_keypair_device.argtypes = [C.c_uint32, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p]
+lib.xmss_b200_sign_open_batch.argtypes = [C.c_int, C.c_uint32, _u8p, _u64p, _u64p, _u8p, C.c_uint32,
+                                          _u32p, _intp]
+lib.xmss_b200_sign_open_device.argtypes = [C.c_uint32, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                           C.c_void_p]
+lib.xmss_b200_sign_batch.argtypes = [C.c_int, C.c_uint32, _u8p, _u8p, _u64p, _u64p, _u8p, _u64p,
+                                     _u64p, _intp]
+lib.xmss_b200_core_hash_batch.argtypes = [C.c_uint, C.c_uint, C.c_uint32, _u8p, _u64p, _u64p, _u8p]
+lib.xmss_b200_last_verify_work.argtypes = [C.POINTER(Work)]
+lib.xmss_b200_profile.argtypes = [C.c_int]
+lib.xmss_b200_phase_ms.argtypes = [C.POINTER(C.c_double)]
+lib.xmss_b200_rate_probe.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
+
+PHASES = ("prep", "chains", "ltree", "root", "tree")
+
+
+def header_functions() -> list[str]:
+    """Names of every function declared in include/*.h."""
+    names = []
+    for f in sorted(os.listdir(INCLUDE_DIR)):
+        if f.endswith(".h"):
+            text = re.sub(r"/\*.*?\*/", "", open(os.path.join(INCLUDE_DIR, f)).read(), flags=re.S)
+            names += re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\([^;{]*\)\s*;", text)
+    return sorted(set(n for n in names if n not in ("if", "while", "for", "return", "sizeof")))
+
+
+def _buf(b, size: int | None = None):
+    if isinstance(b, int):
+        return (C.c_uint8 * max(b, 1))()
+    b = bytes(b)
+    n = max(len(b) if size is None else size, 1)
+    out = (C.c_uint8 * n)()
+    C.memmove(out, b, len(b))
+    return out
+
+
+def _np_ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def last_error() -> str:
+    return lib.xmss_b200_last_error().decode()
+
+
+def _check(ret: int, what: str) -> int:
+    if ret == GPU_FAILURE:
+        raise GpuError(f"{what}: {last_error()}")
+    return ret
+
+
+# -- params.h ----------------------------------------------------------------
+
+def xmss_str_to_oid(name: str) -> int:
+    o = C.c_uint32()
+    if lib.xmss_str_to_oid(C.byref(o), name.encode()):
+        raise ValueError(name)
+    return o.value
+
+
+def xmssmt_str_to_oid(name: str) -> int:
+    o = C.c_uint32()
+    if lib.xmssmt_str_to_oid(C.byref(o), name.encode()):
+        raise ValueError(name)
+    return o.value
+
+
+def parse_oid(oid: int, mt: bool = False) -> XmssParams:
+    p = XmssParams()
+    f = lib.xmssmt_parse_oid if mt else lib.xmss_parse_oid
+    if f(C.byref(p), oid):
+        raise ValueError(f"unknown {'XMSSMT' if mt else 'XMSS'} OID {oid:#x}")
+    return p
+
+
+def params_by_name(name: str) -> tuple[int, bool, XmssParams]:
+    mt = name.startswith("XMSSMT")
+    oid = xmssmt_str_to_oid(name) if mt else xmss_str_to_oid(name)
+    return oid, mt, parse_oid(oid, mt)
+
+
+# -- device / randomness ---------------------------------------------------
+
+def init(device: int = 0) -> None:
+    _check(lib.xmss_b200_init(device), "xmss_b200_init")
+
+
+_rng_keepalive = None
+
+
+def set_randombytes(fn) -> None:
+    """fn(nbytes) -> bytes; None restores /dev/urandom."""
+    global _rng_keepalive
+    if fn is None:
+        _rng_keepalive = None
+        lib.xmss_b200_set_randombytes(_RNG())
+        return
+
+    def cb(x, n):
+        b = fn(n)
+        C.memmove(x, b, n)
+
+    _rng_keepalive = _RNG(cb)
+    lib.xmss_b200_set_randombytes(_rng_keepalive)
+
+
+# -- xmss.h / xmss_core.h ----------------------------------------------------
+
+def _keypair(oid: int, mt: bool):
+    try:
+        p = parse_oid(oid, mt)
+        pkb, skb = XMSS_OID_LEN + p.pk_bytes, XMSS_OID_LEN + p.sk_bytes
+    except ValueError:  # the library answers -1 itself
+        pkb, skb = XMSS_OID_LEN + 128, XMSS_OID_LEN + 8 + 256
+    pk, sk = _buf(pkb), _buf(skb)
+    r = _check((lib.xmssmt_keypair if mt else lib.xmss_keypair)(pk, sk, oid), "keypair")
+    return r, bytes(pk), bytes(sk)
+
+
+def xmss_keypair(oid: int):
+    return _keypair(oid, False)
+
+
+def xmssmt_keypair(oid: int):
+    return _keypair(oid, True)
+
+
+def _sign(sk: bytes, m: bytes, mt: bool):
+    oid = int.from_bytes(sk[:4], "big")
+    try:
+        p = parse_oid(oid, mt)
+        cap = p.sig_bytes + len(m)
+    except ValueError:
+        cap = len(m) + 1
+    skb = _buf(sk)
+    sm = _buf(cap)
+    smlen = C.c_ulonglong()
+    r = _check((lib.xmssmt_sign if mt else lib.xmss_sign)(skb, sm, C.byref(smlen), _buf(m), len(m)), "sign")
+    return r, bytes(skb)[: len(sk)], bytes(sm)[: smlen.value]
+
+
+def xmss_sign(sk: bytes, m: bytes):
+    return _sign(sk, m, False)
+
+
+def xmssmt_sign(sk: bytes, m: bytes):
+    return _sign(sk, m, True)
+
+
+def _sign_open(sm: bytes, pk: bytes, mt: bool):
+    m = _buf(len(sm) + 1)
+    mlen = C.c_ulonglong()
+    r = _check((lib.xmssmt_sign_open if mt else lib.xmss_sign_open)(m, C.byref(mlen), _buf(sm), len(sm),
+                                                                    _buf(pk)), "sign_open")
+    return r, bytes(m)[: mlen.value]
+
+
+def xmss_sign_open(sm: bytes, pk: bytes):
+    return _sign_open(sm, pk, False)
+
+
+def xmssmt_sign_open(sm: bytes, pk: bytes):
+    return _sign_open(sm, pk, True)
+
+
+def xmssmt_core_seed_keypair(p: XmssParams, seed: bytes):
+    pk, sk = _buf(p.pk_bytes), _buf(p.sk_bytes)
+    r = _check(lib.xmssmt_core_seed_keypair(C.byref(p), pk, sk, _buf(seed)), "seed_keypair")
+    return r, bytes(pk), bytes(sk)
+
+
+def xmssmt_core_sign(p: XmssParams, sk: bytes, m: bytes):
+    skb = _buf(sk)
+    sm = _buf(p.sig_bytes + len(m))
+    smlen = C.c_ulonglong()
+    r = _check(lib.xmssmt_core_sign(C.byref(p), skb, sm, C.byref(smlen), _buf(m), len(m)), "core_sign")
+    return r, bytes(skb)[: len(sk)], bytes(sm)[: smlen.value]
+
+
+def xmssmt_core_sign_open(p: XmssParams, sm: bytes, pk: bytes):
+    m = _buf(len(sm) + 1)
+    mlen = C.c_ulonglong()
+    r = _check(lib.xmssmt_core_sign_open(C.byref(p), m, C.byref(mlen), _buf(sm), len(sm), _buf(pk)),
+               "core_sign_open")
+    return r, bytes(m)[: mlen.value]
+
+
+# -- xmss_b200.h batch API ---------------------------------------------------
+
+def keypair_batch(oid: int, mt: bool, seeds: np.ndarray):
+    """seeds: uint8 [count, 3n] -> (pk [count, 4+2n], sk [count, 4+sk_bytes])."""
+    p = parse_oid(oid, mt)
+    seeds = np.ascontiguousarray(seeds, dtype=np.uint8)
+    count = seeds.shape[0]
+    pk = np.zeros((count, XMSS_OID_LEN + p.pk_bytes), np.uint8)
+    sk = np.zeros((count, XMSS_OID_LEN + p.sk_bytes), np.uint8)
+    r = _check(lib.xmss_b200_keypair_batch(oid, int(mt), count, _np_ptr(seeds, C.c_uint8), _np_ptr(pk, C.c_uint8),
+                                           _np_ptr(sk, C.c_uint8)), "keypair_batch")
+    if r:
+        raise ValueError(f"keypair_batch returned {r}")
+    return pk, sk
+
+
+def pack(chunks: Sequence[bytes], align: int = 1):
+    """Concatenates byte strings; returns (buffer uint8, offsets u64, lengths u64)."""
+    offs, lens, pos = [], [], 0
+    for c in chunks:
+        offs.append(pos)
+        lens.append(len(c))
+        pos += (len(c) + align - 1) // align * align
+    buf = np.zeros(max(pos, 1), np.uint8)
+    for o, c in zip(offs, chunks):
+        buf[o:o + len(c)] = np.frombuffer(bytes(c), np.uint8)
+    return buf, np.array(offs, np.uint64), np.array(lens, np.uint64)
+
+
+def sign_open_batch(mt: bool, sm: np.ndarray, sm_off: np.ndarray, smlen: np.ndarray, pk: np.ndarray,
+                    pk_index: np.ndarray | None = None) -> np.ndarray:
+    """Batched xmss[mt]_sign_open; returns int32 status per signed message."""
+    sm = np.ascontiguousarray(sm, np.uint8)
+    sm_off = np.ascontiguousarray(sm_off, np.uint64)
+    smlen = np.ascontiguousarray(smlen, np.uint64)
+    pk = np.ascontiguousarray(pk, np.uint8)
+    count = len(sm_off)
+    status = np.full(count, -7, np.int32)
+    idxp = None
+    if pk_index is not None:
+        pk_index = np.ascontiguousarray(pk_index, np.uint32)
+        idxp = _np_ptr(pk_index, C.c_uint32)
+    r = _check(lib.xmss_b200_sign_open_batch(int(mt), count, _np_ptr(sm, C.c_uint8), _np_ptr(sm_off, C.c_uint64),
+                                             _np_ptr(smlen, C.c_uint64), _np_ptr(pk, C.c_uint8), pk.shape[0],
+                                             idxp, _np_ptr(status, C.c_int)), "sign_open_batch")
+    if r:
+        raise ValueError(f"sign_open_batch returned {r}: {last_error()}")
+    return status
+
+
+def sign_batch(mt: bool, sk: np.ndarray, msgs: Sequence[bytes]):
+    """Batched xmss[mt]_sign.  sk: uint8 [count, 4+sk_bytes], updated in place.
+    Returns (ret int32 [count], list of sm bytes)."""
+    sk = np.ascontiguousarray(sk, np.uint8)
+    count = sk.shape[0]
+    oid = int.from_bytes(bytes(sk[0, :4]), "big")
+    p = parse_oid(oid, mt)
+    mbuf, moff, mlen = pack(msgs)
+    sm_sizes = [p.sig_bytes + len(m) for m in msgs]
+    smbuf, smoff, _ = pack([b"\0" * s for s in sm_sizes])
+    smlen = np.zeros(count, np.uint64)
+    ret = np.zeros(count, np.int32)
+    r = _check(lib.xmss_b200_sign_batch(int(mt), count, _np_ptr(sk, C.c_uint8), _np_ptr(mbuf, C.c_uint8),
+                                        _np_ptr(moff, C.c_uint64), _np_ptr(mlen, C.c_uint64),
+                                        _np_ptr(smbuf, C.c_uint8), _np_ptr(smoff, C.c_uint64),
+                                        _np_ptr(smlen, C.c_uint64), _np_ptr(ret, C.c_int)), "sign_batch")
+    if r:
+        raise ValueError(f"sign_batch returned {r}: {last_error()}")
+    sms = [bytes(smbuf[int(o):int(o) + int(l)]) for o, l in zip(smoff, smlen)]
+    return ret, sms
+
+
+def core_hash_batch(func: int, n: int, msgs: Sequence[bytes]) -> list[bytes]:
+    buf, off, ln = pack(msgs)
+    out = np.zeros((len(msgs), n), np.uint8)
+    r = _check(lib.xmss_b200_core_hash_batch(func, n, len(msgs), _np_ptr(buf, C.c_uint8), _np_ptr(off, C.c_uint64),
+                                             _np_ptr(ln, C.c_uint64), _np_ptr(out, C.c_uint8)), "core_hash_batch")
+    if r:
+        raise ValueError(f"core_hash_batch returned {r}")
+    return [bytes(row) for row in out]
+
+
+def profile(enable: bool) -> None:
+    _check(lib.xmss_b200_profile(int(enable)), "profile")
+
+
+def phase_ms() -> dict:
+    a = (C.c_double * 5)()
+    _check(lib.xmss_b200_phase_ms(a), "phase_ms")
+    return dict(zip(PHASES, list(a)))
+
+
+def rate_probe(kind: int, blocks: int, iters: int, d_sink: int, stream: int = 0) -> None:
+    r = _check(lib.xmss_b200_rate_probe(kind, blocks, iters, d_sink, stream), "rate_probe")
+    if r:
+        raise ValueError(f"rate_probe returned {r}")
+
+
+def last_verify_work() -> Work:
+    w = Work()
+    _check(lib.xmss_b200_last_verify_work(C.byref(w)), "last_verify_work")
+    return w
+
+
+# -- device-pointer API (for callers that keep data in HBM, e.g. torch) -----
+
+def sign_open_device(oid: int, mt: bool, count: int, d_sm: int, d_sm_off: int, d_smlen: int, d_pk: int, npk: int,
+                     d_pk_index: int, d_status: int, stream: int = 0) -> None:
+    r = _check(lib.xmss_b200_sign_open_device(oid, int(mt), count, d_sm, d_sm_off, d_smlen, d_pk, npk, d_pk_index,
+                                              d_status, stream), "sign_open_device")
+    if r:
+        raise ValueError(f"sign_open_device returned {r}: {last_error()}")
+
+
+def keypair_device(oid: int, mt: bool, count: int, d_seeds: int, d_pk: int, d_sk: int, stream: int = 0) -> None:
+    r = _check(lib.xmss_b200_keypair_device(oid, int(mt), count, d_seeds, d_pk, d_sk, stream), "keypair_device")
+    if r:
+        raise ValueError(f"keypair_device returned {r}: {last_error()}")

@@ -1,0 +1,53 @@
+"""The C-ABI library on the CPU: it loads, exports every function that
+include/*.h declares, and its host-side parameter tables match the oracle's
+restatement of params.c for all 77 OIDs.  No GPU compute is called."""
+import ctypes as C
+
+import pytest
+
+
+def test_exports_every_declared_function(xb):
+    declared = xb.header_functions()
+    assert len(declared) >= 30
+    missing = [f for f in declared if not hasattr(xb.lib, f)]
+    assert not missing, missing
+
+
+@pytest.mark.parametrize("mt,count", [(False, 21), (True, 56)])
+def test_params_tables_match_oracle(xb, oracle, mt, count):
+    for oid in range(1, count + 1):
+        assert xb.parse_oid(oid, mt).as_dict() == oracle.params(oid, mt).as_dict(), oid
+    for bad in (0, count + 1, 0xFFFFFFFF):
+        with pytest.raises(ValueError):
+            xb.parse_oid(bad, mt)
+
+
+def test_names_round_trip(xb, oracle):
+    names = ["XMSS-SHA2_10_256", "XMSS-SHAKE_10_256", "XMSS-SHA2_10_512", "XMSS-SHAKE256_20_192",
+             "XMSSMT-SHA2_20/2_256", "XMSSMT-SHA2_40/4_256", "XMSSMT-SHAKE256_60/12_192", "XMSSMT-SHAKE_40/8_512"]
+    for n in names:
+        oid, mt = oracle.str_to_oid(n)
+        assert (xb.xmssmt_str_to_oid(n) if mt else xb.xmss_str_to_oid(n)) == oid
+    with pytest.raises(ValueError):
+        xb.xmss_str_to_oid("XMSS-SHA2_12_256")
+
+
+def test_initialize_params_rejects_bad_w(xb):
+    p = xb.parse_oid(1)
+    p.wots_w = 8
+    assert xb.lib.xmss_xmssmt_initialize_params(C.byref(p)) == -1
+    p.wots_w = 16
+    assert xb.lib.xmss_xmssmt_initialize_params(C.byref(p)) == 0
+    assert xb.lib.xmss_xmssmt_core_sk_bytes(C.byref(p)) == 132
+
+
+def test_every_family_supported(xb):
+    for func, n in ((0, 24), (0, 32), (0, 64), (1, 32), (2, 24), (2, 32), (2, 64)):
+        assert xb.lib.xmss_b200_supported(func, n) == 1
+    assert xb.lib.xmss_b200_supported(1, 64) == 0
+
+
+def test_unknown_oid_rejected_before_gpu(xb):
+    """OID parsing happens on the host: unknown OIDs return -1 like xmss.c."""
+    r, _, _ = xb.xmss_keypair(0x99)
+    assert r == -1

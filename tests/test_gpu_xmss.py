@@ -1,0 +1,170 @@
+"""XMSS / XMSS^MT on the GPU through the C-ABI, byte for byte against the
+reference's own outputs (golden fixtures) and the CPU oracle."""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def h10(b):
+    return hashlib.shake_128(b).hexdigest(10)
+
+
+def test_config1_plain_api(xb, golden):
+    """Config 1: keypair from a seeded 96-byte seed, 16 signatures of 32-byte
+    messages at indices 0..15 through xmss_sign, each verified through
+    xmss_sign_open; pk, sk and every signature byte-identical to the
+    reference C path."""
+    g = golden("config1.json")
+    p = xb.parse_oid(1)
+    r, pk, sk = xb.xmssmt_core_seed_keypair(p, bytes.fromhex(g["seed"]))
+    assert r == 0
+    assert "00000001" + pk.hex() == g["pk"]
+    assert "00000001" + sk.hex() == g["sk"]
+    sk = bytes.fromhex(g["sk"])
+    pkf = bytes.fromhex(g["pk"])
+    for i, m in enumerate(g["msgs"]):
+        m = bytes.fromhex(m)
+        r, sk, sm = xb.xmss_sign(sk, m)
+        assert r == 0
+        assert sm.hex() == g["sms"][i], i
+        assert sk.hex() == g["sk_after"][i]
+        assert xb.xmss_sign_open(sm, pkf) == (0, m)
+        bad = bytearray(sm)
+        bad[-1] ^= 1  # flip the last message bit (test/xmss.c:233-242)
+        assert xb.xmss_sign_open(bytes(bad), pkf) == (-1, b"")
+
+
+def test_invalid_signature_every_hash(xb, golden):
+    """One bit per n-byte hash of the signature, index included
+    (test/xmss.c:244-261, XMSS_TEST_INVALIDSIG), must reject: checked as one
+    batch."""
+    g = golden("config1.json")
+    pk = np.frombuffer(bytes.fromhex(g["pk"]), np.uint8)[None, :]
+    sm = bytes.fromhex(g["sms"][3])
+    mlen = 32
+    variants = []
+    for j in range(0, len(sm) - mlen, 32):
+        b = bytearray(sm)
+        b[j] ^= 1
+        variants.append(bytes(b))
+    variants.append(sm)
+    buf, off, ln = xb.pack(variants)
+    st = xb.sign_open_batch(False, buf, off, ln, pk, np.zeros(len(variants), np.uint32))
+    assert (st[:-1] == -1).all() and st[-1] == 0
+
+
+def test_mt_small_every_family(xb, golden):
+    """XMSS^MT 20/4 keys of all seven hash families: keygen, signature at a
+    given index and verify equal the reference's bytes."""
+    for k in golden("mt_small.json"):
+        p = xb.parse_oid(k["oid"], True)
+        r, pk, sk = xb.xmssmt_core_seed_keypair(p, bytes.fromhex(k["seed"]))
+        assert r == 0 and pk.hex() == k["pk"] and sk.hex() == k["sk"], k["oid"]
+        for s in k["sigs"]:
+            skx = s["idx"].to_bytes(p.index_bytes, "big") + sk[p.index_bytes:]
+            r, sk2, sm = xb.xmssmt_core_sign(p, skx, bytes.fromhex(s["m"]))
+            assert r == 0 and sm.hex() == s["sm"], (k["oid"], s["idx"])
+            assert xb.xmssmt_core_sign_open(p, sm, pk) == (0, bytes.fromhex(s["m"]))
+
+
+def test_reference_vectors_xmss_lines(xb, golden):
+    """The XMSS and XMSS^MT lines of the reference's test/vectors.c
+    (seed[i] = i, signature of {37} at index 2^(h-1)) over every family."""
+    want = [l for l in golden("vectors.txt") if not l.startswith("WOTS")]
+    got = []
+    for mt, oids in ((True, range(2, 57, 8)), (False, range(1, 0x15 + 1, 3))):
+        for oid in oids:
+            p = xb.parse_oid(oid, mt)
+            seed = bytes(i & 0xFF for i in range(3 * p.n))
+            r, pk, sk = xb.xmssmt_core_seed_keypair(p, seed)
+            assert r == 0
+            sk = (1 << (p.full_height - 1)).to_bytes(p.index_bytes, "big") + sk[p.index_bytes:]
+            r, _, sm = xb.xmssmt_core_sign(p, sk, bytes([37]))
+            assert r == 0
+            got.append(f"{'XMSSMT' if mt else 'XMSS'} {oid} {h10(pk)} {h10(sm[:p.sig_bytes])}")
+    assert got == want
+
+
+def test_batch_verify_matches_oracle(xb, oracle):
+    """A mixed batch: several keys, uneven message lengths (0 B..5 KB),
+    random bit flips anywhere in sig || message; accept bitmap == oracle."""
+    rng = np.random.default_rng(5)
+    p = xb.parse_oid(0x01, True)  # XMSSMT-SHA2_20/2_256: two layers of height 10
+    po = oracle.params(0x01, True)
+    seeds = np.frombuffer(rng.bytes(3 * 32 * 3), np.uint8).reshape(3, 96)
+    pks, sks = xb.keypair_batch(0x01, True, seeds)
+    sms, keyix, flips = [], [], []
+    for i in range(24):
+        k = i % 3
+        idx = int(rng.integers(0, 1 << 20))
+        sk = bytes(sks[k, :4]) + idx.to_bytes(p.index_bytes, "big") + bytes(sks[k, 4 + p.index_bytes:])
+        m = rng.bytes(int(rng.integers(0, 5000)))
+        r, _, sm = xb.xmssmt_sign(sk, m)
+        assert r == 0
+        sm = bytearray(sm)
+        if i % 4 == 1:
+            pos = int(rng.integers(0, len(sm)))
+            sm[pos] ^= 1 << int(rng.integers(0, 8))
+        sms.append(bytes(sm))
+        keyix.append(k)
+    buf, off, ln = xb.pack(sms)
+    st = xb.sign_open_batch(True, buf, off, ln, pks, np.array(keyix, np.uint32))
+    want = [oracle.sign_open(po, sm, bytes(pks[k, 4:]))[0] for sm, k in zip(sms, keyix)]
+    assert list(st) == want
+    assert sum(1 for w in want if w == -1) >= 5
+
+
+def test_exhaustion_quirk_matches_oracle(xb, oracle):
+    """xmss_core.c:212-231 at the last index: the wiped key still signs
+    (byte-identical garbage signature), then -2; the sk bytes follow."""
+    p = xb.parse_oid(0x02, True)
+    po = oracle.params(0x02, True)
+    seed = np.random.default_rng(7).bytes(3 * p.n)
+    r, pk, sk = xb.xmssmt_core_seed_keypair(p, seed)
+    last = (1 << p.full_height) - 1
+    sk = last.to_bytes(p.index_bytes, "big") + sk[p.index_bytes:]
+    a = xb.xmssmt_core_sign(p, sk, b"abc")
+    b = oracle.sign(po, sk, b"abc")
+    assert a == b and a[0] == 0
+    a2 = xb.xmssmt_core_sign(p, a[1], b"abc")
+    b2 = oracle.sign(po, b[1], b"abc")
+    assert a2[0] == -2 and a2[:2] == b2[:2]
+    assert a2[2][p.sig_bytes:] == b"abc"
+
+
+def test_determinism_and_empty_message(xb):
+    """Same sk copy signs the same bytes twice (test/xmss_determinism.c);
+    empty messages sign and verify; short sm is rejected."""
+    p = xb.parse_oid(0x02, True)
+    r, pk, sk = xb.xmssmt_core_seed_keypair(p, bytes(range(96)))
+    a = xb.xmssmt_core_sign(p, sk, b"")
+    b = xb.xmssmt_core_sign(p, sk, b"")
+    assert a == b and a[0] == 0 and len(a[2]) == p.sig_bytes
+    assert xb.xmssmt_core_sign_open(p, a[2], pk) == (0, b"")
+    assert xb.xmssmt_core_sign_open(p, a[2][:-1], pk)[0] == -1
+
+
+def test_sign_batch_shares_subtrees(xb, oracle):
+    """Batched signing of consecutive indices of one key (and copies of
+    another) equals one-by-one signing by the oracle."""
+    p = xb.parse_oid(0x02, True)
+    po = oracle.params(0x02, True)
+    rng = np.random.default_rng(9)
+    seeds = np.frombuffer(rng.bytes(2 * 96), np.uint8).reshape(2, 96)
+    pks, sks = xb.keypair_batch(0x02, True, seeds)
+    rows, msgs = [], []
+    for i in range(12):
+        k = i % 2
+        idx = 30 + i
+        rows.append(np.concatenate([sks[k, :4], np.frombuffer(idx.to_bytes(p.index_bytes, "big"), np.uint8),
+                                    sks[k, 4 + p.index_bytes:]]))
+        msgs.append(rng.bytes(int(rng.integers(1, 300))))
+    sk_arr = np.stack(rows)
+    want = [oracle.sign(po, bytes(r[4:]), m) for r, m in zip(sk_arr, msgs)]
+    ret, sms = xb.sign_batch(True, sk_arr, msgs)
+    for i, (w, sm) in enumerate(zip(want, sms)):
+        assert ret[i] == 0 and sm == w[2] and bytes(sk_arr[i, 4:]) == w[1], i
