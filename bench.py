@@ -27,7 +27,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -69,7 +68,9 @@ def make_workload(xb, rank: int = 0):
     ret, sms = xb.sign_batch(False, rows, msgs)
     assert (ret == 0).all()
     flip = rng.choice(NUM_SIGS, NUM_SIGS // 10, replace=False)
-    expect = np.zeros(NUM_SIGS, np.int32)
+    # Index 2^h - 1 is the reference's exhaustion case (xmss_core.c:212-231):
+    # the key is wiped before signing, so that signature must reject.
+    expect = np.where(idx == (1 << p.full_height) - 1, -1, 0).astype(np.int32)
     sms = [bytearray(s) for s in sms]
     for i in flip:
         pos = int(rng.integers(0, len(sms[i])))
@@ -86,60 +87,59 @@ def make_workload(xb, rank: int = 0):
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clock and clock-event reasons polled through NVML every 5 ms during
+    the timed region (started before it; waits for the first sample)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, device: int):
         self.device = device
-        self.proc = None
-        self.lines = []
+        self.samples = []
+        self.stop = threading.Event()
         self.thread = None
+        self.max_mhz = None
+        self.err = None
+
+    def _run(self):
+        try:
+            import pynvml as N
+
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.device)
+            self.max_mhz = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+            while not self.stop.is_set():
+                mhz = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                try:
+                    rs = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                except AttributeError:
+                    rs = N.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                self.samples.append((float(mhz), int(rs)))
+                time.sleep(0.005)
+            N.nvmlShutdown()
+        except Exception as ex:  # NVML missing: report unsampled
+            self.err = str(ex)
 
     def __enter__(self):
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except OSError:
-            self.proc = None
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
+        t0 = time.time()
+        while not self.samples and self.err is None and time.time() - t0 < 5:
+            time.sleep(0.001)
+        self.n0 = len(self.samples)
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-            self.thread.join(timeout=2)
+        self.stop.set()
+        self.thread.join(timeout=5)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
-            f = [x.strip() for x in l.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        s = self.samples[self.n0:] or self.samples
+        if not s:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"], "error": self.err}
+        reasons = sorted({name for _, r in s for bit, name in self.REASONS.items() if r & bit})
+        return {"sm_mhz": float(np.median([m for m, _ in s])), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(s), "source": "NVML, 5 ms"}
 
 
 # ---------------------------------------------------------------------------
@@ -516,7 +516,7 @@ def make_workload_cpu(count: int = 512, keys: int = 8):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--skip-keygen", action="store_true")

@@ -51,7 +51,7 @@ struct Launch {
     static void verify_prep(const VerifyArgs& v, const void* ctx, cudaStream_t st)
     {
         if (!v.count) return;
-        k_verify_prep<F><<<grid_for(v.count), 64, 0, st>>>(v, (const Ctx*)ctx);
+        k_verify_prep<F><<<(v.count + 63) / 64, 64, 0, st>>>(v, (const Ctx*)ctx);
     }
     static void verify_chains(const VerifyArgs& v, uint32_t layer, const void* ctx, cudaStream_t st)
     {

@@ -168,3 +168,31 @@ def test_sign_batch_shares_subtrees(xb, oracle):
     ret, sms = xb.sign_batch(True, sk_arr, msgs)
     for i, (w, sm) in enumerate(zip(want, sms)):
         assert ret[i] == 0 and sm == w[2] and bytes(sk_arr[i, 4:]) == w[1], i
+
+
+def test_sign_batch_long_messages_match_oracle(xb, oracle):
+    """XMSS-SHA2_10_256 batch signing with the benchmark's message-length
+    distribution (log-uniform 32 B..4 KB, unaligned lengths) equals the
+    oracle's signatures, and the batch verify accepts them all."""
+    rng = np.random.default_rng(21)
+    p, po = xb.parse_oid(1), oracle.params(1)
+    seeds = np.frombuffer(rng.bytes(2 * 96), np.uint8).reshape(2, 96)
+    pks, sks = xb.keypair_batch(1, False, seeds)
+    trees = [oracle.tree_nodes(po, bytes(s[:32]), bytes(s[64:]), 0, 0, os.cpu_count()) for s in seeds]
+    for k in range(2):
+        assert bytes(pks[k, 4:36]) == trees[k][-32:]
+    count = 40
+    keyix = rng.integers(0, 2, count)
+    idx = rng.integers(0, 1024, count)
+    mlen = np.exp(rng.uniform(np.log(32), np.log(4096), count)).astype(int)
+    msgs = [rng.bytes(int(L)) for L in mlen]
+    rows = np.array(sks[keyix])
+    for i in range(count):
+        rows[i, 4:8] = np.frombuffer(int(idx[i]).to_bytes(4, "big"), np.uint8)
+    want = [oracle.sign(po, bytes(rows[i, 4:]), msgs[i], trees=trees[keyix[i]]) for i in range(count)]
+    ret, sms = xb.sign_batch(False, rows.copy(), msgs)
+    for i in range(count):
+        assert ret[i] == 0 and sms[i] == want[i][2], (i, int(mlen[i]), int(idx[i]))
+    buf, off, ln = xb.pack(sms, align=16)
+    st = xb.sign_open_batch(False, buf, off, ln, pks, keyix.astype(np.uint32))
+    assert (st == 0).all()
