@@ -278,7 +278,7 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
 {
     XB_CUDA(cudaMemsetAsync(work_, 0, 3 * sizeof(unsigned long long), st));
     if (!count) return;
-    const uint32_t n = p.n, len = ops->len;
+    const uint32_t n = p.n, len = ops->len, nh = len - 1 + p.tree_height;
     void* ctx = s_ctx_.get((size_t)npk * ops->ctx_bytes);
     ops->make_ctx(d_pk + n, 2 * n, nullptr, 0, nullptr, 0, npk, ctx, st);
     VerifyArgs v;
@@ -296,24 +296,39 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
     v.wpk2 = s_wpk2_.as<uint8_t>((size_t)count * ((len + 1) / 2) * n);
     v.leaf = s_leaf_.as<uint8_t>((size_t)count * n);
     v.refs = s_refs_.as<LeafRef>(count);
+    v.hpre = s_hpre_.get((size_t)count * p.d * nh * ops->hpre_bytes);
+    v.hist = s_hist_.as<uint32_t>(32 * p.d);
+    v.list = s_list_.as<uint32_t>((size_t)count * len);
     v.work = work_;
     v.count = count;
     v.index_bytes = p.index_bytes;
     v.sig_bytes = p.sig_bytes;
     v.tree_height = p.tree_height;
     v.d = p.d;
+    XB_CUDA(cudaMemsetAsync(v.hist, 0, 32 * p.d * sizeof(uint32_t), st));
     mark(kPrep, true, st);
     ops->verify_prep(v, ctx, st);
     mark(kPrep, false, st);
     for (uint32_t layer = 0; layer < p.d; layer++) {
         mark(kChains, true, st);
+        ops->verify_scatter(v, layer, st);
         ops->verify_chains(v, layer, ctx, st);
         mark(kChains, false, st);
         mark(kLtree, true, st);
-        run_ltree(ops, v.refs, count, v.wpk, v.wpk2, v.leaf, ctx, v.status, st);
+        int cnt = (int)len;
+        uint32_t node_base = 0;
+        uint8_t *src = v.wpk, *dst = v.wpk2;
+        uint32_t sstr = len, dstr = (len + 1) / 2;
+        while (cnt > 1) {
+            ops->verify_ltree(v, layer, cnt, node_base, src, sstr, dst, dstr, st);
+            node_base += cnt / 2;
+            cnt = (cnt + 1) / 2;
+            std::swap(src, dst);
+            std::swap(sstr, dstr);
+        }
         mark(kLtree, false, st);
         mark(kRoot, true, st);
-        ops->verify_root(v, layer, ctx, st);
+        ops->verify_root(v, layer, st);
         mark(kRoot, false, st);
     }
 }

@@ -133,7 +133,7 @@ class Engine {
     bool have_done_ = false;
     // pipeline scratch
     DevBuf s_ctx_, s_jobs_, s_refs_, s_wpk_, s_wpk2_, s_nodes_, s_keys_, s_node_, s_lens_, s_idx_, s_leaf_,
-        s_work_, s_tree_off_, s_key_idx_, s_mlen_;
+        s_work_, s_tree_off_, s_key_idx_, s_mlen_, s_hpre_, s_hist_, s_list_;
     PinnedBuf h_jobs_;
     unsigned long long* work_ = nullptr;
     struct Mark {

@@ -19,6 +19,13 @@
 //   prf_r               hash.c:70-81 with key = SK_PRF, in = toByte(idx, 32)
 //   hmsg                hash.c:107-120 over a message in global memory
 //   byte_at             byte k of an n-byte value (for base_w)
+//   HPre, h_pre, h_fin  thash_h split in two: h_pre is the part that depends
+//                       only on the address (the three PRFs, and for the
+//                       midstate forms the first core block toByte(1)||key);
+//                       h_fin finishes the hash from (l, r).  Verify computes
+//                       every h_pre of a signature in parallel up front, so
+//                       the serial L-tree / authentication-path steps cost
+//                       h_fin only (2 compressions instead of 6 for SHA-2).
 //
 // For the SHA-2 sets with padding_len = n the first block of PRF, PRF_keygen
 // and the R-PRF is toByte(X, n) || key and is constant per key, so its
@@ -27,6 +34,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include "hashcore.cuh"
 
@@ -217,6 +225,35 @@ struct GenericFam : FamBase<N_, PL_, Core::BE> {
         Core::template digest<PW + 3 * NW, NW>(o, m);
     }
 
+    struct HPre {
+        uint32_t key[NW];
+        uint32_t m1[NW];
+        uint32_t m2[NW];
+    };
+
+    __device__ static void h_pre(HPre& o, const Ctx& c, uint32_t (&a)[8])
+    {
+        a[7] = 0;
+        prf_adrs(o.key, c, a);
+        a[7] = 1;
+        prf_adrs(o.m1, c, a);
+        a[7] = 2;
+        prf_adrs(o.m2, c, a);
+    }
+
+    __device__ static void h_fin(uint32_t (&o)[NW], const HPre& p, const uint32_t (&l)[NW], const uint32_t (&r)[NW])
+    {
+        uint32_t m[PW + 3 * NW];
+        set_pad(m, 1);
+#pragma unroll
+        for (int i = 0; i < NW; i++) {
+            m[PW + i] = p.key[i];
+            m[PW + NW + i] = l[i] ^ p.m1[i];
+            m[PW + 2 * NW + i] = r[i] ^ p.m2[i];
+        }
+        Core::template digest<PW + 3 * NW, NW>(o, m);
+    }
+
     __device__ static void prf_keygen(uint32_t (&o)[NW], const Ctx& c, const uint32_t (&a)[8])
     {
         uint32_t m[PW + 2 * NW + 8];
@@ -389,6 +426,50 @@ struct Sha256N32 : FamBase<32, 32, true> {
         for (int i = 0; i < 8; i++) o[i] = st[i];
     }
 
+    struct HPre {
+        uint32_t c[8];   // state after the first core block toByte(1,32) || key
+        uint32_t m1[8];
+        uint32_t m2[8];
+    };
+
+    __device__ static void h_pre(HPre& o, const Ctx& c, uint32_t (&a)[8])
+    {
+        uint32_t t[8], w[16];
+        a[7] = 0;
+        prf_adrs(t, c, a);
+#pragma unroll
+        for (int i = 0; i < 7; i++) w[i] = 0;
+        w[7] = 1;
+#pragma unroll
+        for (int i = 0; i < 8; i++) w[8 + i] = t[i];
+        sha256_iv(o.c);
+        sha256_compress(o.c, w);
+        a[7] = 1;
+        prf_adrs(o.m1, c, a);
+        a[7] = 2;
+        prf_adrs(o.m2, c, a);
+    }
+
+    // o may alias l or r.
+    __device__ static void h_fin(uint32_t (&o)[8], const HPre& p, const uint32_t (&l)[8], const uint32_t (&r)[8])
+    {
+        uint32_t w[16], st[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            w[i] = l[i] ^ p.m1[i];
+            w[8 + i] = r[i] ^ p.m2[i];
+            st[i] = p.c[i];
+        }
+        sha256_compress(st, w);
+        w[0] = 0x80000000u;
+#pragma unroll
+        for (int i = 1; i < 15; i++) w[i] = 0;
+        w[15] = 1024;
+        sha256_compress(st, w);
+#pragma unroll
+        for (int i = 0; i < 8; i++) o[i] = st[i];
+    }
+
     __device__ static void prf_keygen(uint32_t (&o)[8], const Ctx& c, const uint32_t (&a)[8])
     {
         uint32_t w[16];
@@ -535,6 +616,48 @@ struct Sha512N64 : FamBase<64, 64, true> {
 #pragma unroll
         for (int i = 1; i < 15; i++) w[i] = 0;
         w[15] = 2048;  // 256 * 8
+        sha512_compress(st, w);
+        out16(o, st);
+    }
+
+    struct HPre {
+        uint64_t c[8];  // state after toByte(1,64) || key
+        uint64_t m1[8];
+        uint64_t m2[8];
+    };
+
+    __device__ static void h_pre(HPre& o, const Ctx& c, uint32_t (&a)[8])
+    {
+        uint64_t t[8], w[16];
+        a[7] = 0;
+        prf_adrs(t, c, a);
+#pragma unroll
+        for (int i = 0; i < 7; i++) w[i] = 0;
+        w[7] = 1;
+#pragma unroll
+        for (int i = 0; i < 8; i++) w[8 + i] = t[i];
+        sha512_iv(o.c);
+        sha512_compress(o.c, w);
+        a[7] = 1;
+        prf_adrs(o.m1, c, a);
+        a[7] = 2;
+        prf_adrs(o.m2, c, a);
+    }
+
+    __device__ static void h_fin(uint32_t (&o)[16], const HPre& p, const uint32_t (&l)[16], const uint32_t (&r)[16])
+    {
+        uint64_t st[8], w[16];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            st[i] = p.c[i];
+            w[i] = join64(l[2 * i], l[2 * i + 1]) ^ p.m1[i];
+            w[8 + i] = join64(r[2 * i], r[2 * i + 1]) ^ p.m2[i];
+        }
+        sha512_compress(st, w);
+        w[0] = 0x8000000000000000ull;
+#pragma unroll
+        for (int i = 1; i < 15; i++) w[i] = 0;
+        w[15] = 2048;
         sha512_compress(st, w);
         out16(o, st);
     }
@@ -720,17 +843,109 @@ template <> struct HMsgKind<Shake256N24> { static constexpr int v = 34; };
 template <> struct HMsgKind<Shake256N32> { static constexpr int v = 34; };
 template <> struct HMsgKind<Shake256N64> { static constexpr int v = 34; };
 
+// 16 big-endian words of the 64-byte block at m + o, which lies entirely in
+// [m, m + mlen).  Reads never go past m + mlen; like fetch4_le they may read
+// up to 3 bytes before m + o when it is not 4-byte aligned.
+__device__ __forceinline__ void load_block64_be(uint32_t (&w)[16], const uint8_t* m, uint64_t mlen, uint64_t o)
+{
+    const uint8_t* p = m + o;
+    const uintptr_t a = (uintptr_t)p;
+    if ((a & 15) == 0) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint4 v = __ldg((const uint4*)p + i);
+            w[4 * i] = bswap32(v.x);
+            w[4 * i + 1] = bswap32(v.y);
+            w[4 * i + 2] = bswap32(v.z);
+            w[4 * i + 3] = bswap32(v.w);
+        }
+    } else if ((a & 3) == 0) {
+#pragma unroll
+        for (int i = 0; i < 16; i++) w[i] = bswap32(__ldg((const uint32_t*)p + i));
+    } else if (o + 68 <= mlen) {
+        // 17 aligned words cover the block; the last one ends before m + mlen
+        const uint32_t* q = (const uint32_t*)(a & ~(uintptr_t)3);
+        const int sh = (int)(a & 3) * 8;
+        uint32_t lo = __ldg(q);
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const uint32_t hi = __ldg(q + i + 1);
+            w[i] = bswap32(__funnelshift_r(lo, hi, sh));
+            lo = hi;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 16; i++) w[i] = bswap32(fetch4_le(m, mlen, o + 4 * i));
+    }
+}
+
+// H_msg for SHA-256 with n = 32: the 128-byte prefix is exactly two blocks,
+// so M starts block aligned.  Full message blocks are loaded one block ahead
+// of the compression that consumes them.
+__device__ __forceinline__ void hmsg_sha256_n32(uint32_t (&out)[8], const uint32_t (&R)[8], const uint32_t (&root)[8],
+                                                uint64_t idx, const uint8_t* m, uint64_t mlen)
+{
+    uint32_t st[8], w[16];
+    sha256_iv(st);
+#pragma unroll
+    for (int i = 0; i < 7; i++) w[i] = 0;
+    w[7] = 2;
+#pragma unroll
+    for (int i = 0; i < 8; i++) w[8 + i] = R[i];
+    sha256_compress(st, w);
+#pragma unroll
+    for (int i = 0; i < 8; i++) w[i] = root[i];
+#pragma unroll
+    for (int i = 8; i < 14; i++) w[i] = 0;
+    w[14] = (uint32_t)(idx >> 32);
+    w[15] = (uint32_t)idx;
+    sha256_compress(st, w);
+    const uint64_t nfull = mlen / 64;
+    uint32_t nxt[16];
+    if (nfull) load_block64_be(nxt, m, mlen, 0);
+    for (uint64_t b = 0; b < nfull; b++) {
+#pragma unroll
+        for (int i = 0; i < 16; i++) w[i] = nxt[i];
+        if (b + 1 < nfull) load_block64_be(nxt, m, mlen, 64 * (b + 1));
+        sha256_compress(st, w);
+    }
+    // tail: remaining bytes, 0x80, zero fill, 64-bit bit length of 128 + mlen
+    const uint64_t L = 128 + mlen;
+    const uint64_t o0 = 64 * nfull;
+    const int tail_blocks = ((mlen - o0) + 9 > 64) ? 2 : 1;
+    for (int b = 0; b < tail_blocks; b++) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const uint64_t o = o0 + 64 * b + 4 * j;  // offset into M
+            uint32_t le = (o < mlen) ? fetch4_le(m, mlen, o) : 0;
+            if (o <= mlen && mlen < o + 4) le |= 0x80u << (8 * (mlen - o));
+            w[j] = bswap32(le);
+        }
+        if (b == tail_blocks - 1) {
+            w[14] = (uint32_t)((L * 8) >> 32);
+            w[15] = (uint32_t)(L * 8);
+        }
+        sha256_compress(st, w);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) out[i] = st[i];
+}
+
 template <class F>
 __device__ void hmsg(uint32_t (&out)[F::NW], const uint32_t (&R)[F::NW], const uint32_t (&root)[F::NW],
                      uint64_t idx, const uint8_t* m, uint64_t mlen)
 {
-    HMsgPrefix<F> pre;
-    pre.build(R, root, idx);
-    constexpr int K = HMsgKind<F>::v;
-    if constexpr (K == 0 || K == 1) {
-        HMsgImpl<F, K>::run(out, pre, m, mlen);
+    if constexpr (std::is_same<F, Sha256N32>::value) {
+        hmsg_sha256_n32(out, R, root, idx, m, mlen);
     } else {
-        hmsg_shake<F, K>(out, pre, m, mlen);
+        HMsgPrefix<F> pre;
+        pre.build(R, root, idx);
+        constexpr int K = HMsgKind<F>::v;
+        if constexpr (K == 0 || K == 1) {
+            HMsgImpl<F, K>::run(out, pre, m, mlen);
+        } else {
+            hmsg_shake<F, K>(out, pre, m, mlen);
+        }
     }
 }
 

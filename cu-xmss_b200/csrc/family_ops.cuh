@@ -51,7 +51,15 @@ struct Launch {
     static void verify_prep(const VerifyArgs& v, const void* ctx, cudaStream_t st)
     {
         if (!v.count) return;
-        k_verify_prep<F><<<(v.count + 63) / 64, 64, 0, st>>>(v, (const Ctx*)ctx);
+        const uint32_t hb = (v.count + 63) / 64;
+        const uint64_t pre = (uint64_t)v.count * v.d * (F::LEN - 1 + v.tree_height);
+        k_verify_prep<F><<<(unsigned)(hb + (pre + 63) / 64), 64, 0, st>>>(v, hb, (const Ctx*)ctx);
+    }
+    static void verify_scatter(const VerifyArgs& v, uint32_t layer, cudaStream_t st)
+    {
+        const uint64_t items = (uint64_t)v.count * F::LEN;
+        if (!items) return;
+        k_verify_scatter<F><<<(unsigned)((items + 255) / 256), 256, 0, st>>>(v, layer);
     }
     static void verify_chains(const VerifyArgs& v, uint32_t layer, const void* ctx, cudaStream_t st)
     {
@@ -59,10 +67,19 @@ struct Launch {
         if (!items) return;
         k_verify_chains<F><<<grid_for(items), kBlock, 0, st>>>(v, layer, (const Ctx*)ctx);
     }
-    static void verify_root(const VerifyArgs& v, uint32_t layer, const void* ctx, cudaStream_t st)
+    static void verify_ltree(const VerifyArgs& v, uint32_t layer, int cnt_in, uint32_t node_base,
+                             const uint8_t* src, uint32_t src_stride, uint8_t* dst, uint32_t dst_stride,
+                             cudaStream_t st)
+    {
+        const uint64_t items = (uint64_t)v.count * ((cnt_in + 1) / 2);
+        if (!items) return;
+        k_verify_ltree<F><<<grid_for(items), kBlock, 0, st>>>(v, layer, cnt_in, node_base, src, src_stride, dst,
+                                                              dst_stride);
+    }
+    static void verify_root(const VerifyArgs& v, uint32_t layer, cudaStream_t st)
     {
         if (!v.count) return;
-        k_verify_root<F><<<(v.count + 63) / 64, 64, 0, st>>>(v, layer, (const Ctx*)ctx);
+        k_verify_root<F><<<(v.count + 63) / 64, 64, 0, st>>>(v, layer);
     }
     static void sign_prep(const SignArgs& g, const void* ctx, cudaStream_t st)
     {
@@ -84,9 +101,26 @@ struct Launch {
 
     static FamilyOps table(const char* name, unsigned func)
     {
-        return FamilyOps{name,          func,          (unsigned)F::N, (unsigned)F::LEN, sizeof(Ctx),
-                         make_ctx,      keygen_chains, ltree_level,    tree_level,       verify_prep,
-                         verify_chains, verify_root,   sign_prep,      sign_chains,      core_hash};
+        FamilyOps o{};
+        o.name = name;
+        o.func = func;
+        o.n = (unsigned)F::N;
+        o.len = (unsigned)F::LEN;
+        o.ctx_bytes = sizeof(Ctx);
+        o.make_ctx = make_ctx;
+        o.keygen_chains = keygen_chains;
+        o.ltree_level = ltree_level;
+        o.tree_level = tree_level;
+        o.hpre_bytes = sizeof(typename F::HPre);
+        o.verify_prep = verify_prep;
+        o.verify_scatter = verify_scatter;
+        o.verify_chains = verify_chains;
+        o.verify_ltree = verify_ltree;
+        o.verify_root = verify_root;
+        o.sign_prep = sign_prep;
+        o.sign_chains = sign_chains;
+        o.core_hash = core_hash;
+        return o;
     }
 };
 

@@ -27,9 +27,13 @@ struct FamilyOps {
                         const int* status, cudaStream_t st);
     void (*tree_level)(const TreeJob* jobs, uint32_t njobs, int h, int level, uint8_t* nodes, const void* ctx,
                        cudaStream_t st);
+    size_t hpre_bytes;  // sizeof(F::HPre)
     void (*verify_prep)(const VerifyArgs& v, const void* ctx, cudaStream_t st);
+    void (*verify_scatter)(const VerifyArgs& v, uint32_t layer, cudaStream_t st);
     void (*verify_chains)(const VerifyArgs& v, uint32_t layer, const void* ctx, cudaStream_t st);
-    void (*verify_root)(const VerifyArgs& v, uint32_t layer, const void* ctx, cudaStream_t st);
+    void (*verify_ltree)(const VerifyArgs& v, uint32_t layer, int cnt_in, uint32_t node_base, const uint8_t* src,
+                         uint32_t src_stride, uint8_t* dst, uint32_t dst_stride, cudaStream_t st);
+    void (*verify_root)(const VerifyArgs& v, uint32_t layer, cudaStream_t st);
     void (*sign_prep)(const SignArgs& g, const void* ctx, cudaStream_t st);
     void (*sign_chains)(const SignArgs& g, const void* ctx, cudaStream_t st);
     void (*core_hash)(const uint8_t* msgs, const uint64_t* off, const uint64_t* len, uint32_t count, uint8_t* out,

@@ -14,11 +14,47 @@ namespace xb {
 __device__ __forceinline__ uint32_t ror32(uint32_t x, int n) { return __funnelshift_r(x, x, n); }
 __device__ __forceinline__ uint32_t bswap32(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
 
+// Pipe balancing.  SHA-256 here is bound by the integer ALU pipe (rotates,
+// LOP3 and IADD3 all issue there) while the FMA pipe idles.  An integer
+// multiply-add with a multiplier the compiler cannot see (read from constant
+// memory, always 1 at run time) executes on the FMA pipe, so additions
+// written as a * one + b move off the ALU pipe; right shifts by k likewise
+// become mul.hi by 2^(32-k).  Results are bit-identical.
+static __constant__ uint32_t xb_pipe_one = 1u;
+static __constant__ uint32_t xb_pipe_pow2[33] = {
+    0u,        1u << 1,  1u << 2,  1u << 3,  1u << 4,  1u << 5,  1u << 6,  1u << 7,  1u << 8,
+    1u << 9,   1u << 10, 1u << 11, 1u << 12, 1u << 13, 1u << 14, 1u << 15, 1u << 16, 1u << 17,
+    1u << 18,  1u << 19, 1u << 20, 1u << 21, 1u << 22, 1u << 23, 1u << 24, 1u << 25, 1u << 26,
+    1u << 27,  1u << 28, 1u << 29, 1u << 30, 1u << 31, 0u};
+
+__device__ __forceinline__ uint32_t fma_add(uint32_t a, uint32_t b)
+{
+    uint32_t r;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(xb_pipe_one), "r"(b));
+    return r;
+}
+
+// x >> k for 0 < k < 32 on the FMA pipe
+template <int K>
+__device__ __forceinline__ uint32_t fma_shr(uint32_t x)
+{
+    uint32_t r;
+    asm("mul.hi.u32 %0, %1, %2;" : "=r"(r) : "r"(x), "r"(xb_pipe_pow2[32 - K]));
+    return r;
+}
+
 // ---------------------------------------------------------------------------
 // SHA-256 compression (FIPS 180-4 6.2.2).  `w` is consumed (message schedule
-// is expanded in place in a 16-word window).
+// is expanded in place in a 16-word window).  MIX selects how the work is
+// spread over the ALU and FMA pipes: 0 all on ALU, 1 the additions on FMA,
+// 2 additions and the schedule's right shifts on FMA.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void sha256_compress(uint32_t (&st)[8], uint32_t (&w)[16])
+#ifndef XB_SHA256_MIX
+#define XB_SHA256_MIX 1
+#endif
+
+template <int MIX>
+__device__ __forceinline__ void sha256_compress_t(uint32_t (&st)[8], uint32_t (&w)[16])
 {
     const uint32_t K[64] = {
         0x428a2f98u, 0x71374491u, 0xb5c0fbcfu, 0xe9b5dba5u, 0x3956c25bu, 0x59f111f1u,
@@ -38,20 +74,39 @@ __device__ __forceinline__ void sha256_compress(uint32_t (&st)[8], uint32_t (&w)
     for (int t = 0; t < 64; t++) {
         if (t >= 16) {
             const uint32_t x15 = w[(t - 15) & 15], x2 = w[(t - 2) & 15];
-            const uint32_t s0 = ror32(x15, 7) ^ ror32(x15, 18) ^ (x15 >> 3);
-            const uint32_t s1 = ror32(x2, 17) ^ ror32(x2, 19) ^ (x2 >> 10);
-            w[t & 15] += s0 + w[(t - 7) & 15] + s1;
+            if constexpr (MIX == 0) {
+                const uint32_t s0 = ror32(x15, 7) ^ ror32(x15, 18) ^ (x15 >> 3);
+                const uint32_t s1 = ror32(x2, 17) ^ ror32(x2, 19) ^ (x2 >> 10);
+                w[t & 15] += s0 + w[(t - 7) & 15] + s1;
+            } else {
+                const uint32_t r0 = (MIX == 2) ? fma_shr<3>(x15) : (x15 >> 3);
+                const uint32_t r1 = (MIX == 2) ? fma_shr<10>(x2) : (x2 >> 10);
+                const uint32_t s0 = ror32(x15, 7) ^ ror32(x15, 18) ^ r0;
+                const uint32_t s1 = ror32(x2, 17) ^ ror32(x2, 19) ^ r1;
+                w[t & 15] = fma_add(s1, fma_add(s0, w[t & 15] + w[(t - 7) & 15]));
+            }
         }
         const uint32_t S1 = ror32(e, 6) ^ ror32(e, 11) ^ ror32(e, 25);
         const uint32_t ch = g ^ (e & (f ^ g));
-        const uint32_t t1 = h + S1 + ch + K[t] + w[t & 15];
         const uint32_t S0 = ror32(a, 2) ^ ror32(a, 13) ^ ror32(a, 22);
         const uint32_t mj = (a & b) | (c & (a | b));
-        h = g; g = f; f = e; e = d + t1;
-        d = c; c = b; b = a; a = t1 + S0 + mj;
+        if constexpr (MIX == 0) {
+            const uint32_t t1 = h + S1 + ch + K[t] + w[t & 15];
+            h = g; g = f; f = e; e = d + t1;
+            d = c; c = b; b = a; a = t1 + S0 + mj;
+        } else {
+            const uint32_t t1 = fma_add(ch, fma_add(S1, h + K[t] + w[t & 15]));
+            h = g; g = f; f = e; e = fma_add(d, t1);
+            d = c; c = b; b = a; a = fma_add(S0, fma_add(mj, t1));
+        }
     }
     st[0] += a; st[1] += b; st[2] += c; st[3] += d;
     st[4] += e; st[5] += f; st[6] += g; st[7] += h;
+}
+
+__device__ __forceinline__ void sha256_compress(uint32_t (&st)[8], uint32_t (&w)[16])
+{
+    sha256_compress_t<XB_SHA256_MIX>(st, w);
 }
 
 __device__ __forceinline__ void sha256_iv(uint32_t (&st)[8])

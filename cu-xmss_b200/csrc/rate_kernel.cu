@@ -9,6 +9,7 @@
 
 namespace xb {
 
+template <int MIX>
 __global__ void __launch_bounds__(128) k_sha256_rate(uint32_t iters, uint32_t seed, uint32_t* __restrict__ sink)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -24,7 +25,7 @@ __global__ void __launch_bounds__(128) k_sha256_rate(uint32_t iters, uint32_t se
             w[j] = st[j];
             w[8 + j] = st[j] ^ i;
         }
-        sha256_compress(st, w);
+        sha256_compress_t<MIX>(st, w);
     }
     uint32_t x = 0;
 #pragma unroll
@@ -49,12 +50,18 @@ __global__ void __launch_bounds__(128) k_keccak_rate(uint32_t iters, uint32_t se
     if ((uint32_t)x == 0x9E3779B9u) sink[t] = (uint32_t)x;
 }
 
+// kind 0: SHA-256 as the XMSS kernels compile it; 1: Keccak-f[1600];
+// 10 + m: SHA-256 with pipe mix m (for comparing the variants).
 void launch_rate(int kind, uint32_t blocks, uint32_t iters, uint32_t* sink, cudaStream_t st)
 {
-    if (kind == 0)
-        k_sha256_rate<<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink);
-    else
-        k_keccak_rate<<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink);
+    switch (kind) {
+        case 0: k_sha256_rate<XB_SHA256_MIX><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 1: k_keccak_rate<<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 10: k_sha256_rate<0><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 11: k_sha256_rate<1><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 12: k_sha256_rate<2><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
+        default: break;
+    }
 }
 
 }  // namespace xb

@@ -203,6 +203,13 @@ __global__ void __launch_bounds__(128) k_tree_level(const TreeJob* __restrict__ 
 
 // ---------------------------------------------------------------------------
 // Verify (xmss_commons.c:136-215).
+//
+// Per layer the work is: chains (wots_pk_from_sig), L-tree (66 H for n=32),
+// compute_root (h H).  Every H is split into h_pre (address only) and h_fin
+// (data dependent); all h_pre of all layers run in the prep launch next to
+// H_msg, so the dependent L-tree / root steps are 2 compressions each.  The
+// chains are bucketed by their number of F steps (15 - len_i) and run
+// longest first, so each warp runs chains of equal length.
 // ---------------------------------------------------------------------------
 struct VerifyArgs {
     const uint8_t* sm;        // concatenated signed messages
@@ -219,7 +226,10 @@ struct VerifyArgs {
     uint8_t* wpk2;            // [count][LEN/2 + 1][N]
     uint8_t* leaf;            // [count][N]
     LeafRef* refs;            // [count]
-    unsigned long long* work;  // [3] H_msg blocks, F calls, H calls (accumulated)
+    void* hpre;               // [count][d][NH] F::HPre, NH = LEN - 1 + tree_height
+    uint32_t* hist;           // [d][32]: chains per step count, then bucket cursors
+    uint32_t* list;           // [count * LEN] chain work list, longest first
+    unsigned long long* work; // [3] H_msg blocks, F calls, H calls (accumulated)
     uint32_t count;
     uint32_t index_bytes;
     uint32_t sig_bytes;
@@ -238,60 +248,176 @@ __device__ __forceinline__ unsigned long long hmsg_blocks(uint64_t mlen)
     else return L / (4 * K) + 1;
 }
 
+// Adds the step counts of one signature's chains to a block histogram.
 template <class F>
-__device__ __forceinline__ unsigned long long chain_steps(const uint8_t* lens)
+__device__ __forceinline__ unsigned long long count_steps(const uint8_t* lens, uint32_t* sh_hist)
 {
     unsigned long long s = 0;
-    for (int i = 0; i < F::LEN; i++) s += 15 - lens[i];
+    for (int i = 0; i < F::LEN; i++) {
+        const uint32_t steps = 15 - lens[i];
+        s += steps;
+        atomicAdd(&sh_hist[steps], 1u);
+    }
     return s;
 }
 
-template <class F>
-__global__ void k_verify_prep(VerifyArgs v, const typename F::Ctx* __restrict__ ctx)
+__device__ __forceinline__ void flush_hist(uint32_t* sh_hist, uint32_t* hist)
 {
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= v.count) return;
-    const uint64_t smlen = v.smlen[s];
-    if (smlen < v.sig_bytes) {  // the reference would underflow here; reject
-        v.status[s] = -1;
+    __syncthreads();
+    if (threadIdx.x < 16 && sh_hist[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh_hist[threadIdx.x]);
+}
+
+template <class F>
+__device__ __forceinline__ void layer_addr(uint64_t idx, uint32_t th, uint32_t layer, uint32_t& leaf, uint64_t& tree)
+{
+    leaf = (uint32_t)((idx >> (th * layer)) & ((1ull << th) - 1));
+    tree = (th * (layer + 1) >= 64) ? 0 : idx >> (th * (layer + 1));
+}
+
+// Launch = [hmsg_blocks x 64 threads: one signature each] followed by
+// [pre blocks: one (signature, layer, H node) each].  The H nodes of a layer
+// are numbered L-tree level by level (level 0 pairs first), then the h
+// authentication-path levels.
+template <class F>
+__global__ void __launch_bounds__(64) k_verify_prep(VerifyArgs v, uint32_t hmsg_blocks_n,
+                                                    const typename F::Ctx* __restrict__ ctx)
+{
+    using HPre = typename F::HPre;
+    __shared__ uint32_t sh_hist[16];
+    if (blockIdx.x < hmsg_blocks_n) {
+        if (threadIdx.x < 16) sh_hist[threadIdx.x] = 0;
+        __syncthreads();
+        const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+        if (s < v.count) {
+            const uint64_t smlen = v.smlen[s];
+            if (smlen < v.sig_bytes) {  // the reference would underflow here; reject
+                v.status[s] = -1;
+            } else {
+                const uint8_t* sm = v.sm + v.sm_off[s];
+                const uint64_t idx = bytes_be(sm, (int)v.index_bytes);
+                uint32_t R[F::NW], root[F::NW], mh[F::NW];
+                F::load(R, sm + v.index_bytes);
+                F::load(root, v.key_root + (uint64_t)v.key[s] * v.key_stride);
+                hmsg<F>(mh, R, root, idx, sm + v.sig_bytes, smlen - v.sig_bytes);
+                F::store(v.node + (uint64_t)s * F::N, mh);
+                uint8_t* lens = v.lens + (uint64_t)s * F::LEN;
+                chain_lengths<F>(lens, mh);
+                v.idx[s] = idx;
+                v.status[s] = 0;
+                const unsigned long long steps = count_steps<F>(lens, sh_hist);
+                if (v.work) {
+                    atomicAdd(&v.work[0], hmsg_blocks<F>(smlen - v.sig_bytes));
+                    atomicAdd(&v.work[1], steps);
+                    atomicAdd(&v.work[2], (unsigned long long)(F::LEN - 1 + v.tree_height) * v.d);
+                }
+            }
+        }
+        flush_hist(sh_hist, v.hist);
         return;
     }
-    const uint8_t* sm = v.sm + v.sm_off[s];
-    const uint64_t idx = bytes_be(sm, (int)v.index_bytes);
-    uint32_t R[F::NW], root[F::NW], mh[F::NW];
-    F::load(R, sm + v.index_bytes);
-    F::load(root, v.key_root + (uint64_t)v.key[s] * v.key_stride);
-    hmsg<F>(mh, R, root, idx, sm + v.sig_bytes, smlen - v.sig_bytes);
-    F::store(v.node + (uint64_t)s * F::N, mh);
-    uint8_t* lens = v.lens + (uint64_t)s * F::LEN;
-    chain_lengths<F>(lens, mh);
-    v.idx[s] = idx;
-    v.status[s] = 0;
-    if (v.work) {
-        atomicAdd(&v.work[0], hmsg_blocks<F>(smlen - v.sig_bytes));
-        atomicAdd(&v.work[1], chain_steps<F>(lens));
-        atomicAdd(&v.work[2], (unsigned long long)(F::LEN - 1 + v.tree_height) * v.d);
+    const uint32_t nh = F::LEN - 1 + v.tree_height;
+    const uint64_t item = (uint64_t)(blockIdx.x - hmsg_blocks_n) * blockDim.x + threadIdx.x;
+    if (item >= (uint64_t)v.count * v.d * nh) return;
+    const uint32_t s = (uint32_t)(item / ((uint64_t)v.d * nh));
+    const uint32_t rem = (uint32_t)(item - (uint64_t)s * v.d * nh);
+    const uint32_t layer = rem / nh;
+    uint32_t node = rem - layer * nh;
+    if (v.smlen[s] < v.sig_bytes) return;
+    const uint64_t idx = bytes_be(v.sm + v.sm_off[s], (int)v.index_bytes);
+    uint32_t leaf;
+    uint64_t tree;
+    layer_addr<F>(idx, v.tree_height, layer, leaf, tree);
+    uint32_t a[8];
+    if (node < F::LEN - 1) {
+        // locate (level, pair) of L-tree node `node`
+        int cnt = F::LEN, level = 0;
+        while (node >= (uint32_t)(cnt >> 1)) {
+            node -= cnt >> 1;
+            cnt = (cnt + 1) >> 1;
+            level++;
+        }
+        set_addr(a, layer, tree, ADDR_LTREE, leaf, (uint32_t)level, node);
+    } else {
+        const uint32_t i = node - (F::LEN - 1);
+        set_addr(a, layer, tree, ADDR_HASHTREE, 0, i, leaf >> (i + 1));
+    }
+    HPre hp;
+    F::h_pre(hp, ctx[v.key[s]], a);
+    ((HPre*)v.hpre)[item] = hp;
+}
+
+// Buckets the chains of one layer by step count (longest first) into
+// v.list; zero-step chains are copied straight to the WOTS pk.  Also writes
+// the L-tree address of every signature.
+template <class F>
+__global__ void __launch_bounds__(256) k_verify_scatter(VerifyArgs v, uint32_t layer)
+{
+    __shared__ uint32_t sh_cnt[16], sh_base[16];
+    uint32_t* hist = v.hist + 32 * layer;
+    if (threadIdx.x < 16) sh_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = item < (uint64_t)v.count * F::LEN;
+    const uint32_t s = in ? (uint32_t)(item / F::LEN) : 0;
+    const uint32_t chain = in ? (uint32_t)(item - (uint64_t)s * F::LEN) : 0;
+    const bool live = in && v.status[s] == 0;
+    uint32_t steps = 0, local = 0;
+    if (live) {
+        steps = 15 - v.lens[item];
+        if (steps) local = atomicAdd(&sh_cnt[steps], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 16) {
+        const uint32_t k = threadIdx.x;
+        uint32_t base = 0;
+        for (uint32_t j = k + 1; j < 16; j++) base += hist[j];  // longer chains first
+        sh_base[k] = sh_cnt[k] ? base + atomicAdd(&hist[16 + k], sh_cnt[k]) : 0;
+    }
+    __syncthreads();
+    if (!live) return;
+    const uint32_t th = v.tree_height;
+    const uint64_t wsb = (uint64_t)F::LEN * F::N;
+    if (steps) {
+        v.list[sh_base[steps] + local] = (uint32_t)item;
+    } else {
+        const uint8_t* sig = v.sm + v.sm_off[s] + v.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N);
+        uint32_t x[F::NW];
+        F::load(x, sig + (uint64_t)chain * F::N);
+        F::store(v.wpk + item * F::N, x);
+    }
+    if (chain == 0) {
+        LeafRef r;
+        layer_addr<F>(v.idx[s], th, layer, r.leaf, r.tree);
+        r.key = v.key[s];
+        r.layer = layer;
+        r.pad = 0;
+        r.out_off = (uint64_t)s * F::N;
+        v.refs[s] = r;
     }
 }
 
-// One thread per (signature, chain): gen_chain(len_i, w-1-len_i) of
+// One thread per listed chain: gen_chain(len_i, w-1-len_i) of
 // wots_pk_from_sig (wots.c:161-175).
 template <class F>
 __global__ void __launch_bounds__(128) k_verify_chains(VerifyArgs v, uint32_t layer,
                                                        const typename F::Ctx* __restrict__ ctx)
 {
-    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (item >= (uint64_t)v.count * F::LEN) return;
-    const uint32_t s = (uint32_t)(item / F::LEN);
-    const uint32_t chain = (uint32_t)(item - (uint64_t)s * F::LEN);
-    if (v.status[s] != 0) return;
-    const uint64_t idx = v.idx[s];
-    const uint32_t th = v.tree_height;
-    const uint32_t leaf = (uint32_t)((idx >> (th * layer)) & ((1ull << th) - 1));
-    const uint64_t tree = (th * (layer + 1) >= 64) ? 0 : idx >> (th * (layer + 1));
-    const uint32_t start = v.lens[(uint64_t)s * F::LEN + chain];
+    const uint32_t* hist = v.hist + 32 * layer;
+    uint32_t total = 0;
+#pragma unroll
+    for (int k = 1; k < 16; k++) total += hist[k];
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const uint32_t item = v.list[t];
+    const uint32_t s = item / F::LEN;
+    const uint32_t chain = item - s * F::LEN;
+    uint32_t leaf;
+    uint64_t tree;
+    layer_addr<F>(v.idx[s], v.tree_height, layer, leaf, tree);
+    const uint32_t start = v.lens[item];
     const uint64_t wsb = (uint64_t)F::LEN * F::N;
-    const uint8_t* sig = v.sm + v.sm_off[s] + v.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N);
+    const uint8_t* sig =
+        v.sm + v.sm_off[s] + v.index_bytes + F::N + layer * (wsb + (uint64_t)v.tree_height * F::N);
     uint32_t x[F::NW], a[8];
     F::load(x, sig + (uint64_t)chain * F::N);
     set_addr(a, layer, tree, ADDR_OTS, leaf, chain, 0);
@@ -301,61 +427,94 @@ __global__ void __launch_bounds__(128) k_verify_chains(VerifyArgs v, uint32_t la
         a[6] = i;
         F::thash_f(x, c, a);
     }
-    F::store(v.wpk + item * F::N, x);
-    if (chain == 0) {
-        LeafRef r;
-        r.key = v.key[s];
-        r.layer = layer;
-        r.tree = tree;
-        r.leaf = leaf;
-        r.pad = 0;
-        r.out_off = (uint64_t)s * F::N;
-        v.refs[s] = r;
+    F::store(v.wpk + (uint64_t)item * F::N, x);
+}
+
+// One L-tree level of one layer with precomputed h_pre: item = (sig, pair).
+template <class F>
+__global__ void __launch_bounds__(128) k_verify_ltree(VerifyArgs v, uint32_t layer, int cnt_in, uint32_t node_base,
+                                                      const uint8_t* __restrict__ src, uint32_t src_stride,
+                                                      uint8_t* __restrict__ dst, uint32_t dst_stride)
+{
+    using HPre = typename F::HPre;
+    const int pairs = (cnt_in + 1) >> 1;
+    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= (uint64_t)v.count * pairs) return;
+    const uint32_t s = (uint32_t)(item / pairs);
+    const int p = (int)(item - (uint64_t)s * pairs);
+    if (v.status[s] != 0) return;
+    const uint8_t* sp = src + ((uint64_t)s * src_stride) * F::N;
+    uint8_t* out = (cnt_in == 2) ? v.leaf + (uint64_t)s * F::N : dst + ((uint64_t)s * dst_stride + p) * F::N;
+    uint32_t l[F::NW], r[F::NW], o[F::NW];
+    F::load(l, sp + (uint64_t)(2 * p) * F::N);
+    if (2 * p + 1 < cnt_in) {
+        F::load(r, sp + (uint64_t)(2 * p + 1) * F::N);
+        const uint32_t nh = F::LEN - 1 + v.tree_height;
+        const HPre& hp = ((const HPre*)v.hpre)[((uint64_t)s * v.d + layer) * nh + node_base + p];
+        F::h_fin(o, hp, l, r);
+        F::store(out, o);
+    } else {
+        F::store(out, l);
     }
 }
 
-// compute_root (xmss_commons.c:54-96) for one layer; then either the next
-// layer's chain lengths or the final comparison with the public root.
+// compute_root (xmss_commons.c:54-96) for one layer with precomputed h_pre;
+// then either the next layer's chain lengths or the comparison with the
+// public root (xmss_commons.c:204-209).
 template <class F>
-__global__ void k_verify_root(VerifyArgs v, uint32_t layer, const typename F::Ctx* __restrict__ ctx)
+__global__ void __launch_bounds__(64) k_verify_root(VerifyArgs v, uint32_t layer)
 {
+    using HPre = typename F::HPre;
+    __shared__ uint32_t sh_hist[16];
+    if (threadIdx.x < 16) sh_hist[threadIdx.x] = 0;
+    __syncthreads();
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= v.count || v.status[s] != 0) return;
-    const uint64_t idx = v.idx[s];
-    const uint32_t th = v.tree_height;
-    uint32_t leafidx = (uint32_t)((idx >> (th * layer)) & ((1ull << th) - 1));
-    const uint64_t tree = (th * (layer + 1) >= 64) ? 0 : idx >> (th * (layer + 1));
-    const uint64_t wsb = (uint64_t)F::LEN * F::N;
-    const uint8_t* auth =
-        v.sm + v.sm_off[s] + v.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N) + wsb;
-    const typename F::Ctx& c = ctx[v.key[s]];
-    uint32_t cur[F::NW], sib[F::NW], a[8];
-    F::load(cur, v.leaf + (uint64_t)s * F::N);
+    if (s < v.count && v.status[s] == 0) {
+        const uint32_t th = v.tree_height;
+        uint32_t leafidx;
+        uint64_t tree;
+        layer_addr<F>(v.idx[s], th, layer, leafidx, tree);
+        const uint64_t wsb = (uint64_t)F::LEN * F::N;
+        const uint8_t* auth = v.sm + v.sm_off[s] + v.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N) + wsb;
+        const uint32_t nh = F::LEN - 1 + th;
+        const HPre* hp = (const HPre*)v.hpre + ((uint64_t)s * v.d + layer) * nh + (F::LEN - 1);
+        uint32_t cur[F::NW], sib[F::NW], nsib[F::NW];
+        F::load(cur, v.leaf + (uint64_t)s * F::N);
+        F::load(sib, auth);
+        HPre h = hp[0], hnext;
 #pragma unroll 1
-    for (uint32_t i = 0; i < th; i++) {
-        F::load(sib, auth + (uint64_t)i * F::N);
-        const uint32_t odd = leafidx & 1;
-        leafidx >>= 1;
-        set_addr(a, layer, tree, ADDR_HASHTREE, 0, i, leafidx);
-        if (odd) {
-            F::thash_h(cur, sib, cur, c, a);
+        for (uint32_t i = 0; i < th; i++) {
+            // fetch the next level's operands while this level hashes
+            if (i + 1 < th) {
+                hnext = hp[i + 1];
+                F::load(nsib, auth + (uint64_t)(i + 1) * F::N);
+            }
+            if (leafidx & 1) {
+                F::h_fin(cur, h, sib, cur);
+            } else {
+                F::h_fin(cur, h, cur, sib);
+            }
+            leafidx >>= 1;
+            h = hnext;
+#pragma unroll
+            for (int k = 0; k < F::NW; k++) sib[k] = nsib[k];
+        }
+        if (layer + 1 < v.d) {
+            F::store(v.node + (uint64_t)s * F::N, cur);
+            uint8_t* lens = v.lens + (uint64_t)s * F::LEN;
+            chain_lengths<F>(lens, cur);
+            const unsigned long long st = count_steps<F>(lens, sh_hist);
+            if (v.work) atomicAdd(&v.work[1], st);
         } else {
-            F::thash_h(cur, cur, sib, c, a);
+            uint32_t pr[F::NW];
+            F::load(pr, v.key_root + (uint64_t)v.key[s] * v.key_stride);
+            uint32_t diff = 0;
+#pragma unroll
+            for (int i = 0; i < F::NW; i++) diff |= pr[i] ^ cur[i];
+            v.status[s] = diff ? -1 : 0;
         }
     }
-    if (layer + 1 < v.d) {
-        F::store(v.node + (uint64_t)s * F::N, cur);
-        uint8_t* lens = v.lens + (uint64_t)s * F::LEN;
-        chain_lengths<F>(lens, cur);
-        if (v.work) atomicAdd(&v.work[1], chain_steps<F>(lens));
-    } else {
-        uint32_t pr[F::NW];
-        F::load(pr, v.key_root + (uint64_t)v.key[s] * v.key_stride);
-        uint32_t diff = 0;
-#pragma unroll
-        for (int i = 0; i < F::NW; i++) diff |= pr[i] ^ cur[i];
-        v.status[s] = diff ? -1 : 0;
-    }
+    if (layer + 1 < v.d) flush_hist(sh_hist, v.hist + 32 * (layer + 1));
 }
 
 // ---------------------------------------------------------------------------
