@@ -274,6 +274,12 @@ int sign_open_api(uint8_t* m, unsigned long long* mlen, const uint8_t* sm, unsig
 
 }  // namespace
 
+namespace xb {
+// Lets other translation units of the library report through
+// xmss_b200_last_error.
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace xb
+
 // ===========================================================================
 // randombytes.h
 // ===========================================================================

@@ -110,6 +110,22 @@ int xmss_b200_last_verify_work(xmss_b200_work *out);
 int xmss_b200_profile(int enable);
 int xmss_b200_phase_ms(double ms[5]);
 
+/* Same as xmss_b200_sign_open_device, but allocates nothing: no
+ * reference counterpart; it exists for callers that cannot allocate device
+ * memory when they verify (a request path that cannot absorb cudaMalloc's
+ * device synchronisation and latency, or a process held to a fixed device
+ * memory budget).  Its intermediate buffers live in one fixed 8 MiB array in
+ * device memory that every GPU using the library holds until exit; a batch
+ * that does not fit returns -1 (XMSS-SHA2_10_256 fits up to about 760
+ * signatures per call).
+ * All calls share that array: calls whose GPU work overlaps race, so callers
+ * serialise them.  The first call on each device looks the array up with
+ * that device current and should come before any stream capture. */
+int xmss_b200_sign_open_device_noalloc(uint32_t oid, int mt, uint32_t count, const uint8_t *d_sm,
+                                       const uint64_t *d_sm_off, const uint64_t *d_smlen,
+                                       const uint8_t *d_pk, uint32_t npk, const uint32_t *d_pk_index,
+                                       int *d_status, void *stream);
+
 /* Compression-rate probe (the roofline denominator): `blocks` x 128 threads
  * each run `iters` dependent SHA-256 compressions (kind 0) or Keccak-f[1600]
  * permutations (kind 1) in registers, on `stream`.  d_sink: blocks x 128
