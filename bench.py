@@ -220,18 +220,22 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     xb.profile(False)
     med = {k: float(np.median([ph[k] for ph in phases])) for k in phases[0]}
 
-    # ---- compression-rate probe (roofline denominator) ----
+    # ---- compression-rate probe (roofline denominator): the best of the
+    # plain (ALU pipe) and FMA-pipe forms of the SHA-256 compression ----
     probe_blocks = 148 * 16 * 4
     iters = 2000
     sink = torch.zeros(probe_blocks * 128, dtype=torch.int32, device=dev)
-    xb.rate_probe(0, probe_blocks, 50, sink.data_ptr(), sh)
-    torch.cuda.synchronize()
-    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    pe0.record(stream)
-    xb.rate_probe(0, probe_blocks, iters, sink.data_ptr(), sh)
-    pe1.record(stream)
-    torch.cuda.synchronize()
-    probe_rate = probe_blocks * 128 * iters / (pe0.elapsed_time(pe1) / 1e3)
+    probe = {}
+    for kind in (10, 11):
+        xb.rate_probe(kind, probe_blocks, 50, sink.data_ptr(), sh)
+        torch.cuda.synchronize()
+        pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        pe0.record(stream)
+        xb.rate_probe(kind, probe_blocks, iters, sink.data_ptr(), sh)
+        pe1.record(stream)
+        torch.cuda.synchronize()
+        probe[kind] = probe_blocks * 128 * iters / (pe0.elapsed_time(pe1) / 1e3)
+    probe_rate = max(probe.values())
 
     # ---- e2e through the host-buffer C-ABI ----
     h_sm = torch.from_numpy(w["buf"]).pin_memory().numpy()
@@ -301,7 +305,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                      "peak": probe_rate / 1e9, "unit": "Gcompr/s", "frac": achieved / (probe_rate / 1e9),
                      "traffic": traffic,
                      "peak_source": "measured in this run: rate probe, 4 x 148 x 16 CTAs of 128 threads x "
-                                    f"{iters} SHA-256 compressions (same core as the kernels)",
+                                    f"{iters} SHA-256 compressions (same core as the kernels), best of the "
+                                    "ALU-pipe and FMA-pipe forms",
+                     "probe_gcompr_s": {"alu_form": probe[10] / 1e9, "fma_form": probe[11] / 1e9},
                      "work_per_launch": {"compressions": comp_chain, "f_calls": work.f_calls},
                      "phase_ms": med,
                      "pipeline_gcompr_s": pipeline_rate,

@@ -316,14 +316,30 @@ using Shake256N64 = GenericFam<CoreShake<34>, 64, 64>;
 // ---------------------------------------------------------------------------
 // SHA-256, n = 32, padding_len = 32: midstate form.
 // ---------------------------------------------------------------------------
-struct Sha256N32 : FamBase<32, 32, true> {
-    struct Ctx {
-        uint32_t pub[8];
-        uint32_t sks[8];
-        uint32_t prf_mid[8];  // compress(IV, toByte(3,32) || PUB_SEED)
-        uint32_t kg_mid[8];   // compress(IV, toByte(4,32) || SK_SEED)
-        uint32_t r_mid[8];    // compress(IV, toByte(3,32) || SK_PRF)
-    };
+struct Sha256N32Ctx {
+    uint32_t pub[8];
+    uint32_t sks[8];
+    uint32_t prf_mid[8];  // compress(IV, toByte(3,32) || PUB_SEED)
+    uint32_t kg_mid[8];   // compress(IV, toByte(4,32) || SK_SEED)
+    uint32_t r_mid[8];    // compress(IV, toByte(3,32) || SK_PRF)
+};
+
+struct Sha256N32HPre {
+    uint32_t c[8];   // state after the first core block toByte(1,32) || key
+    uint32_t m1[8];
+    uint32_t m2[8];
+};
+
+// MIX is the SHA-256 pipe mix (hashcore.cuh): kernels that keep many warps
+// busy use the FMA-pipe form, serial / latency-bound ones the plain form.
+template <int MIX>
+struct Sha256N32T : FamBase<32, 32, true> {
+    using Ctx = Sha256N32Ctx;
+    using HPre = Sha256N32HPre;
+    __device__ __forceinline__ static void compress(uint32_t (&st)[8], uint32_t (&w)[16])
+    {
+        sha256_compress_t<MIX>(st, w);
+    }
 
     __device__ __forceinline__ static void mid(uint32_t (&st)[8], uint32_t x, const uint32_t (&k)[8])
     {
@@ -334,7 +350,7 @@ struct Sha256N32 : FamBase<32, 32, true> {
 #pragma unroll
         for (int i = 0; i < 8; i++) w[8 + i] = k[i];
         sha256_iv(st);
-        sha256_compress(st, w);
+        compress(st, w);
     }
 
     __device__ static void make_ctx(Ctx& c, const uint8_t* pub, const uint8_t* sks, const uint8_t* skp)
@@ -365,7 +381,7 @@ struct Sha256N32 : FamBase<32, 32, true> {
 #pragma unroll
         for (int i = 9; i < 15; i++) w[i] = 0;
         w[15] = 768;
-        sha256_compress(out, w);
+        compress(out, w);
     }
 
     __device__ static void thash_f(uint32_t (&x)[8], const Ctx& c, uint32_t (&a)[8])
@@ -375,7 +391,7 @@ struct Sha256N32 : FamBase<32, 32, true> {
         prf_adrs(t, c, a);  // mask
 #pragma unroll
         for (int i = 0; i < 8; i++) x[i] ^= t[i];
-        a[7] = 0;
+        a[7] = after(0, t[7]);  // key PRF strictly after the mask PRF
         prf_adrs(key, c, a);
 #pragma unroll
         for (int i = 0; i < 8; i++) {
@@ -383,14 +399,14 @@ struct Sha256N32 : FamBase<32, 32, true> {
             w[8 + i] = key[i];
         }
         sha256_iv(t);
-        sha256_compress(t, w);
+        compress(t, w);
 #pragma unroll
         for (int i = 0; i < 8; i++) w[i] = x[i];
         w[8] = 0x80000000u;
 #pragma unroll
         for (int i = 9; i < 15; i++) w[i] = 0;
         w[15] = 768;
-        sha256_compress(t, w);
+        compress(t, w);
 #pragma unroll
         for (int i = 0; i < 8; i++) x[i] = t[i];
     }
@@ -407,7 +423,7 @@ struct Sha256N32 : FamBase<32, 32, true> {
 #pragma unroll
         for (int i = 0; i < 8; i++) w[8 + i] = t[i];
         sha256_iv(st);
-        sha256_compress(st, w);
+        compress(st, w);
         a[7] = 1;
         prf_adrs(t, c, a);
 #pragma unroll
@@ -416,21 +432,15 @@ struct Sha256N32 : FamBase<32, 32, true> {
         prf_adrs(t, c, a);
 #pragma unroll
         for (int i = 0; i < 8; i++) w[8 + i] = r[i] ^ t[i];
-        sha256_compress(st, w);
+        compress(st, w);
         w[0] = 0x80000000u;
 #pragma unroll
         for (int i = 1; i < 15; i++) w[i] = 0;
         w[15] = 1024;
-        sha256_compress(st, w);
+        compress(st, w);
 #pragma unroll
         for (int i = 0; i < 8; i++) o[i] = st[i];
     }
-
-    struct HPre {
-        uint32_t c[8];   // state after the first core block toByte(1,32) || key
-        uint32_t m1[8];
-        uint32_t m2[8];
-    };
 
     __device__ static void h_pre(HPre& o, const Ctx& c, uint32_t (&a)[8])
     {
@@ -443,7 +453,7 @@ struct Sha256N32 : FamBase<32, 32, true> {
 #pragma unroll
         for (int i = 0; i < 8; i++) w[8 + i] = t[i];
         sha256_iv(o.c);
-        sha256_compress(o.c, w);
+        compress(o.c, w);
         a[7] = 1;
         prf_adrs(o.m1, c, a);
         a[7] = 2;
@@ -460,12 +470,12 @@ struct Sha256N32 : FamBase<32, 32, true> {
             w[8 + i] = r[i] ^ p.m2[i];
             st[i] = p.c[i];
         }
-        sha256_compress(st, w);
+        compress(st, w);
         w[0] = 0x80000000u;
 #pragma unroll
         for (int i = 1; i < 15; i++) w[i] = 0;
         w[15] = 1024;
-        sha256_compress(st, w);
+        compress(st, w);
 #pragma unroll
         for (int i = 0; i < 8; i++) o[i] = st[i];
     }
@@ -479,12 +489,94 @@ struct Sha256N32 : FamBase<32, 32, true> {
             w[8 + i] = a[i];
             o[i] = c.kg_mid[i];
         }
-        sha256_compress(o, w);
+        compress(o, w);
         w[0] = 0x80000000u;
 #pragma unroll
         for (int i = 1; i < 15; i++) w[i] = 0;
         w[15] = 1024;
-        sha256_compress(o, w);
+        compress(o, w);
+    }
+
+    // A whole WOTS chain in one loop over compression sub-steps, so the kernel
+    // holds a single copy of the (fully unrolled, ~1,400-instruction)
+    // compression: with the four compressions of F inlined separately the
+    // chain loop no longer fits the instruction cache.  With keygen, the chain
+    // starts with PRF_keygen (2 sub-steps, hash.c:87-98) from the address in
+    // `a` (hash = key_and_mask = 0); then `steps` F calls at hash addresses
+    // start .. start + steps - 1, 4 sub-steps each: mask PRF, key PRF,
+    // toByte(0) || key, (x ^ mask) || padding (hash.c:157-183).
+    static constexpr bool kHasChain = true;
+
+    __device__ static void chain(uint32_t (&x)[8], const Ctx& c, const uint32_t (&a)[8], uint32_t start,
+                                 uint32_t steps, bool keygen)
+    {
+        uint32_t tmp[8];  // key, then the state after toByte(0) || key
+        const uint32_t pre = keygen ? 2 : 0;
+        const uint32_t total = pre + 4 * steps;
+#pragma unroll 1
+        for (uint32_t j = 0; j < total; j++) {
+            uint32_t st[8], w[16];
+            const uint32_t jj = j - pre;
+            const uint32_t phase = (j < pre) ? 4 + j : (jj & 3);
+            const uint32_t hash = start + (jj >> 2);
+            if (phase <= 1) {  // PRF(PUB_SEED, ADRS) with key_and_mask 1 (mask), then 0 (key)
+#pragma unroll
+                for (int i = 0; i < 6; i++) w[i] = a[i];
+                w[6] = hash;
+                w[7] = 1 - phase;
+                w[8] = 0x80000000u;
+#pragma unroll
+                for (int i = 9; i < 15; i++) w[i] = 0;
+                w[15] = 768;
+#pragma unroll
+                for (int i = 0; i < 8; i++) st[i] = c.prf_mid[i];
+            } else if (phase == 2) {  // toByte(0, 32) || key from the IV
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    w[i] = 0;
+                    w[8 + i] = tmp[i];
+                }
+                sha256_iv(st);
+            } else if (phase == 3) {  // (x ^ mask) || padding of 96 bytes
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    w[i] = x[i];
+                    st[i] = tmp[i];
+                }
+                w[8] = 0x80000000u;
+#pragma unroll
+                for (int i = 9; i < 15; i++) w[i] = 0;
+                w[15] = 768;
+            } else if (phase == 4) {  // PRF_keygen: PUB_SEED || ADRS from the SK_SEED midstate
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    w[i] = c.pub[i];
+                    st[i] = c.kg_mid[i];
+                }
+#pragma unroll
+                for (int i = 0; i < 6; i++) w[8 + i] = a[i];
+                w[14] = 0;
+                w[15] = 0;
+            } else {  // PRF_keygen padding block (128 bytes)
+#pragma unroll
+                for (int i = 0; i < 8; i++) st[i] = x[i];
+                w[0] = 0x80000000u;
+#pragma unroll
+                for (int i = 1; i < 15; i++) w[i] = 0;
+                w[15] = 1024;
+            }
+            compress(st, w);
+            if (phase == 0) {
+#pragma unroll
+                for (int i = 0; i < 8; i++) x[i] ^= st[i];
+            } else if (phase <= 2) {
+#pragma unroll
+                for (int i = 0; i < 8; i++) tmp[i] = st[i];
+            } else {
+#pragma unroll
+                for (int i = 0; i < 8; i++) x[i] = st[i];
+            }
+        }
     }
 
     __device__ static void prf_r(uint32_t (&o)[8], const Ctx& c, uint64_t idx)
@@ -500,9 +592,12 @@ struct Sha256N32 : FamBase<32, 32, true> {
         w[15] = 768;
 #pragma unroll
         for (int i = 0; i < 8; i++) o[i] = c.r_mid[i];
-        sha256_compress(o, w);
+        compress(o, w);
     }
 };
+
+using Sha256N32 = Sha256N32T<0>;
+using Sha256N32Fma = Sha256N32T<1>;
 
 // ---------------------------------------------------------------------------
 // SHA-512, n = 64, padding_len = 64: midstate form over 64-bit words.
@@ -835,7 +930,7 @@ __device__ void hmsg_shake(uint32_t (&out)[F::NW], const HMsgPrefix<F>& pre, con
 }
 
 template <class F> struct HMsgKind;
-template <> struct HMsgKind<Sha256N32> { static constexpr int v = 0; };
+template <int M> struct HMsgKind<Sha256N32T<M>> { static constexpr int v = 0; };
 template <> struct HMsgKind<Sha256N24> { static constexpr int v = 0; };
 template <> struct HMsgKind<Sha512N64> { static constexpr int v = 1; };
 template <> struct HMsgKind<Shake128N32> { static constexpr int v = 42; };
@@ -935,7 +1030,7 @@ template <class F>
 __device__ void hmsg(uint32_t (&out)[F::NW], const uint32_t (&R)[F::NW], const uint32_t (&root)[F::NW],
                      uint64_t idx, const uint8_t* m, uint64_t mlen)
 {
-    if constexpr (std::is_same<F, Sha256N32>::value) {
+    if constexpr (std::is_same<typename F::Ctx, Sha256N32Ctx>::value) {
         hmsg_sha256_n32(out, R, root, idx, m, mlen);
     } else {
         HMsgPrefix<F> pre;

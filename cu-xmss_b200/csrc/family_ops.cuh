@@ -14,9 +14,12 @@ inline unsigned grid_for(uint64_t items)
     return (unsigned)((items + kBlock - 1) / kBlock);
 }
 
-template <class F>
+// F runs every kernel except the chain kernels, which run FT (the same
+// family with another SHA-256 pipe mix; Ctx and HPre are shared).
+template <class F, class FT = F>
 struct Launch {
     using Ctx = typename F::Ctx;
+    static_assert(sizeof(typename FT::Ctx) == sizeof(Ctx), "chain family must share the key context");
 
     static void make_ctx(const uint8_t* pub, uint32_t pub_stride, const uint8_t* sks, uint32_t sks_stride,
                          const uint8_t* skp, uint32_t skp_stride, uint32_t nkeys, void* ctx, cudaStream_t st)
@@ -30,7 +33,8 @@ struct Launch {
     {
         const uint64_t items = nslots * F::LEN;
         if (!items) return;
-        k_keygen_chains<F><<<grid_for(items), kBlock, 0, st>>>(jobs, h, slot0, nslots, (const Ctx*)ctx, wpk, refs);
+        k_keygen_chains<FT>
+            <<<grid_for(items), kBlock, 0, st>>>(jobs, h, slot0, nslots, (const typename FT::Ctx*)ctx, wpk, refs);
     }
     static void ltree_level(const LeafRef* refs, uint32_t nslots, int level, int cnt_in, const uint8_t* src,
                             uint32_t src_stride, uint8_t* dst, uint32_t dst_stride, uint8_t* leaf_out,
@@ -65,7 +69,7 @@ struct Launch {
     {
         const uint64_t items = (uint64_t)v.count * F::LEN;
         if (!items) return;
-        k_verify_chains<F><<<grid_for(items), kBlock, 0, st>>>(v, layer, (const Ctx*)ctx);
+        k_verify_chains<FT><<<grid_for(items), kBlock, 0, st>>>(v, layer, (const typename FT::Ctx*)ctx);
     }
     static void verify_ltree(const VerifyArgs& v, uint32_t layer, int cnt_in, uint32_t node_base,
                              const uint8_t* src, uint32_t src_stride, uint8_t* dst, uint32_t dst_stride,
@@ -90,7 +94,7 @@ struct Launch {
     {
         const uint64_t items = (uint64_t)g.count * g.d * F::LEN;
         if (!items) return;
-        k_sign_chains<F><<<grid_for(items), kBlock, 0, st>>>(g, (const Ctx*)ctx);
+        k_sign_chains<FT><<<grid_for(items), kBlock, 0, st>>>(g, (const typename FT::Ctx*)ctx);
     }
     static void core_hash(const uint8_t* msgs, const uint64_t* off, const uint64_t* len, uint32_t count,
                           uint8_t* out, cudaStream_t st)

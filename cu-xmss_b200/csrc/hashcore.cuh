@@ -21,6 +21,17 @@ __device__ __forceinline__ uint32_t bswap32(uint32_t x) { return __byte_perm(x, 
 // written as a * one + b move off the ALU pipe; right shifts by k likewise
 // become mul.hi by 2^(32-k).  Results are bit-identical.
 static __constant__ uint32_t xb_pipe_one = 1u;
+static __constant__ uint32_t xb_pipe_zero = 0u;
+
+// v | (dep & 0) with a zero the compiler cannot see: makes v depend on dep,
+// which keeps two otherwise independent compressions from being interleaved
+// (each interleaved compression holds another ~24 registers).
+__device__ __forceinline__ uint32_t after(uint32_t v, uint32_t dep)
+{
+    uint32_t r;
+    asm("and.b32 %0, %1, %2;" : "=r"(r) : "r"(dep), "r"(xb_pipe_zero));
+    return v | r;
+}
 static __constant__ uint32_t xb_pipe_pow2[33] = {
     0u,        1u << 1,  1u << 2,  1u << 3,  1u << 4,  1u << 5,  1u << 6,  1u << 7,  1u << 8,
     1u << 9,   1u << 10, 1u << 11, 1u << 12, 1u << 13, 1u << 14, 1u << 15, 1u << 16, 1u << 17,
@@ -47,10 +58,13 @@ __device__ __forceinline__ uint32_t fma_shr(uint32_t x)
 // SHA-256 compression (FIPS 180-4 6.2.2).  `w` is consumed (message schedule
 // is expanded in place in a 16-word window).  MIX selects how the work is
 // spread over the ALU and FMA pipes: 0 all on ALU, 1 the additions on FMA,
-// 2 additions and the schedule's right shifts on FMA.
+// 2 additions and the schedule's right shifts on FMA; 3 is the ALU form
+// re-associated for latency: e' = (d + h + K + W) + S1 + Ch and
+// a' = ((h + K + W) + S0 + Maj) + S1 + Ch, so each round has three dependent
+// levels (rotate, xor, add) on both the a and the e path instead of four.
 // ---------------------------------------------------------------------------
 #ifndef XB_SHA256_MIX
-#define XB_SHA256_MIX 1
+#define XB_SHA256_MIX 0
 #endif
 
 template <int MIX>
@@ -74,7 +88,7 @@ __device__ __forceinline__ void sha256_compress_t(uint32_t (&st)[8], uint32_t (&
     for (int t = 0; t < 64; t++) {
         if (t >= 16) {
             const uint32_t x15 = w[(t - 15) & 15], x2 = w[(t - 2) & 15];
-            if constexpr (MIX == 0) {
+            if constexpr (MIX == 0 || MIX == 3) {
                 const uint32_t s0 = ror32(x15, 7) ^ ror32(x15, 18) ^ (x15 >> 3);
                 const uint32_t s1 = ror32(x2, 17) ^ ror32(x2, 19) ^ (x2 >> 10);
                 w[t & 15] += s0 + w[(t - 7) & 15] + s1;
@@ -94,6 +108,12 @@ __device__ __forceinline__ void sha256_compress_t(uint32_t (&st)[8], uint32_t (&
             const uint32_t t1 = h + S1 + ch + K[t] + w[t & 15];
             h = g; g = f; f = e; e = d + t1;
             d = c; c = b; b = a; a = t1 + S0 + mj;
+        } else if constexpr (MIX == 3) {
+            const uint32_t hkw = h + K[t] + w[t & 15];
+            const uint32_t dhkw = d + hkw;
+            const uint32_t s1c = S1 + ch;
+            h = g; g = f; f = e; e = dhkw + s1c;
+            d = c; c = b; b = a; a = (hkw + S0 + mj) + s1c;
         } else {
             const uint32_t t1 = fma_add(ch, fma_add(S1, h + K[t] + w[t & 15]));
             h = g; g = f; f = e; e = fma_add(d, t1);

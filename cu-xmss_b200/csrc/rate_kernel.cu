@@ -51,10 +51,15 @@ __global__ void __launch_bounds__(128) k_keccak_rate(uint32_t iters, uint32_t se
 }
 
 // kind 0: SHA-256 as the XMSS kernels compile it; 1: Keccak-f[1600];
-// 10 + m: SHA-256 with pipe mix m (for comparing the variants).
+// 10 + m: SHA-256 with pipe mix m (for comparing the variants);
+// 20 + m: the same with one warp per block (latency of a lone thread).
 void launch_rate(int kind, uint32_t blocks, uint32_t iters, uint32_t* sink, cudaStream_t st)
 {
     switch (kind) {
+        case 13: k_sha256_rate<3><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 20: k_sha256_rate<0><<<blocks, 32, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 21: k_sha256_rate<1><<<blocks, 32, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 23: k_sha256_rate<3><<<blocks, 32, 0, st>>>(iters, 0x1234567u, sink); break;
         case 0: k_sha256_rate<XB_SHA256_MIX><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
         case 1: k_keccak_rate<<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
         case 10: k_sha256_rate<0><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;

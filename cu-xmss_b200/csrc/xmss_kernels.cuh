@@ -16,6 +16,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include "families.cuh"
 
@@ -89,6 +90,32 @@ __device__ __forceinline__ void chain_lengths(uint8_t* lens, const uint32_t (&ms
 
 // Per-key contexts from strided rows of PUB_SEED, SK_SEED and SK_PRF (the
 // secret rows may be absent for verify-only keys).
+// WOTS chain: optional PRF_keygen (expand_seed, wots.c:14-29) then F at hash
+// addresses start .. start+steps-1 (gen_chain, wots.c:38-53).  Families with
+// a fused chain loop (F::kHasChain) run it; others call their hashes.
+template <class F, class = void>
+struct HasChain : std::false_type {};
+template <class F>
+struct HasChain<F, std::void_t<decltype(F::kHasChain)>> : std::true_type {};
+
+template <class F>
+__device__ __forceinline__ void run_chain(uint32_t (&x)[F::NW], const typename F::Ctx& c, uint32_t (&a)[8],
+                                          uint32_t start, uint32_t steps, bool keygen)
+{
+    if constexpr (HasChain<F>::value) {
+        F::chain(x, c, a, start, steps, keygen);
+    } else {
+        if (keygen) F::prf_keygen(x, c, a);
+#pragma unroll 1
+        for (uint32_t i = start; i < start + steps; i++) {
+            a[6] = i;
+            F::thash_f(x, c, a);
+        }
+    }
+}
+
+// Per-key contexts from strided rows of PUB_SEED, SK_SEED and SK_PRF (the
+// secret rows may be absent for verify-only keys).
 template <class F>
 __global__ void k_make_ctx(const uint8_t* __restrict__ pub, uint32_t pub_stride, const uint8_t* __restrict__ sks,
                            uint32_t sks_stride, const uint8_t* __restrict__ skp, uint32_t skp_stride,
@@ -126,12 +153,7 @@ __global__ void __launch_bounds__(128) k_keygen_chains(const TreeJob* __restrict
     const typename F::Ctx& c = ctx[job.key];
     uint32_t a[8], x[F::NW];
     set_addr(a, job.layer, job.tree, ADDR_OTS, leaf, chain, 0);
-    F::prf_keygen(x, c, a);
-#pragma unroll 1
-    for (uint32_t i = 0; i < 15; i++) {
-        a[6] = i;
-        F::thash_f(x, c, a);
-    }
+    run_chain<F>(x, c, a, 0, 15, true);
     F::store(wpk + item * F::N, x);
     if (chain == 0) {
         LeafRef r;
@@ -421,12 +443,7 @@ __global__ void __launch_bounds__(128) k_verify_chains(VerifyArgs v, uint32_t la
     uint32_t x[F::NW], a[8];
     F::load(x, sig + (uint64_t)chain * F::N);
     set_addr(a, layer, tree, ADDR_OTS, leaf, chain, 0);
-    const typename F::Ctx& c = ctx[v.key[s]];
-#pragma unroll 1
-    for (uint32_t i = start; i < 15; i++) {
-        a[6] = i;
-        F::thash_f(x, c, a);
-    }
+    run_chain<F>(x, ctx[v.key[s]], a, start, 15 - start, false);
     F::store(v.wpk + (uint64_t)item * F::N, x);
 }
 
@@ -489,11 +506,16 @@ __global__ void __launch_bounds__(64) k_verify_root(VerifyArgs v, uint32_t layer
                 hnext = hp[i + 1];
                 F::load(nsib, auth + (uint64_t)(i + 1) * F::N);
             }
-            if (leafidx & 1) {
-                F::h_fin(cur, h, sib, cur);
-            } else {
-                F::h_fin(cur, h, cur, sib);
+            // the node goes right when its index is odd (xmss_commons.c:61-69);
+            // select operands instead of branching so a warp runs one path
+            const bool odd = leafidx & 1;
+            uint32_t l[F::NW], r[F::NW];
+#pragma unroll
+            for (int k = 0; k < F::NW; k++) {
+                l[k] = odd ? sib[k] : cur[k];
+                r[k] = odd ? cur[k] : sib[k];
             }
+            F::h_fin(cur, h, l, r);
             leafidx >>= 1;
             h = hnext;
 #pragma unroll
@@ -516,6 +538,7 @@ __global__ void __launch_bounds__(64) k_verify_root(VerifyArgs v, uint32_t layer
     }
     if (layer + 1 < v.d) flush_hist(sh_hist, v.hist + 32 * (layer + 1));
 }
+
 
 // ---------------------------------------------------------------------------
 // Sign (xmss_core.c:183-273) given built subtrees.
@@ -595,12 +618,7 @@ __global__ void __launch_bounds__(128) k_sign_chains(SignArgs g, const typename 
     const typename F::Ctx& c = ctx[g.key[s]];
     uint32_t x[F::NW], a[8];
     set_addr(a, layer, tree, ADDR_OTS, leaf, chain, 0);
-    F::prf_keygen(x, c, a);
-#pragma unroll 1
-    for (uint32_t i = 0; i < steps; i++) {
-        a[6] = i;
-        F::thash_f(x, c, a);
-    }
+    run_chain<F>(x, c, a, 0, steps, true);
     const uint64_t wsb = (uint64_t)F::LEN * F::N;
     uint8_t* sig = g.sm + g.sm_off[s] + g.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N);
     F::store(sig + (uint64_t)chain * F::N, x);

@@ -22,7 +22,8 @@ from typing import Sequence
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libxmss_b200.so")
+# XMSS_B200_LIB selects another build of the library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("XMSS_B200_LIB") or os.path.join(HERE, "libxmss_b200.so")
 INCLUDE_DIR = os.path.join(os.path.dirname(os.path.dirname(HERE)), "include")
 
 XMSS_SHA2, XMSS_SHAKE128, XMSS_SHAKE256 = 0, 1, 2
