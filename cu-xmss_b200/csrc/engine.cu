@@ -117,7 +117,10 @@ Engine::Engine(int device) : device_(device)
     if (device < 0 || device >= n) throw CudaFailure("no CUDA device " + std::to_string(device));
     XB_CUDA(cudaSetDevice(device));
     XB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    XB_CUDA(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking));
     XB_CUDA(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming));
+    XB_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+    XB_CUDA(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
     work_ = s_work_.as<unsigned long long>(4);
     XB_CUDA(cudaMemset(work_, 0, 4 * sizeof(unsigned long long)));
 }
@@ -272,40 +275,12 @@ void Engine::keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count,
     XB_CUDA(cudaStreamSynchronize(st));
 }
 
-void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_sm,
-                    const uint64_t* d_sm_off, const uint64_t* d_smlen, const uint8_t* d_pk, uint32_t npk,
-                    const uint32_t* d_pk_index, int* d_status, cudaStream_t st)
+// One launch sequence of verify (prep, then per layer: bucket, chains, L-tree,
+// root) over the signatures v selects, on stream st.
+void Engine::verify_sequence(const FamilyOps* ops, const xmss_params& p, const VerifyArgs& v, const void* ctx,
+                             cudaStream_t st)
 {
-    XB_CUDA(cudaMemsetAsync(work_, 0, 3 * sizeof(unsigned long long), st));
-    if (!count) return;
-    const uint32_t n = p.n, len = ops->len, nh = len - 1 + p.tree_height;
-    void* ctx = s_ctx_.get((size_t)npk * ops->ctx_bytes);
-    ops->make_ctx(d_pk + n, 2 * n, nullptr, 0, nullptr, 0, npk, ctx, st);
-    VerifyArgs v;
-    v.sm = d_sm;
-    v.sm_off = d_sm_off;
-    v.smlen = d_smlen;
-    v.key = d_pk_index;
-    v.key_root = d_pk;
-    v.key_stride = 2 * n;
-    v.node = s_node_.as<uint8_t>((size_t)count * n);
-    v.lens = s_lens_.as<uint8_t>((size_t)count * len);
-    v.idx = s_idx_.as<uint64_t>(count);
-    v.status = d_status;
-    v.wpk = s_wpk_.as<uint8_t>((size_t)count * len * n);
-    v.wpk2 = s_wpk2_.as<uint8_t>((size_t)count * ((len + 1) / 2) * n);
-    v.leaf = s_leaf_.as<uint8_t>((size_t)count * n);
-    v.refs = s_refs_.as<LeafRef>(count);
-    v.hpre = s_hpre_.get((size_t)count * p.d * nh * ops->hpre_bytes);
-    v.hist = s_hist_.as<uint32_t>(32 * p.d);
-    v.list = s_list_.as<uint32_t>((size_t)count * len);
-    v.work = work_;
-    v.count = count;
-    v.index_bytes = p.index_bytes;
-    v.sig_bytes = p.sig_bytes;
-    v.tree_height = p.tree_height;
-    v.d = p.d;
-    XB_CUDA(cudaMemsetAsync(v.hist, 0, 32 * p.d * sizeof(uint32_t), st));
+    const uint32_t len = ops->len;
     mark(kPrep, true, st);
     ops->verify_prep(v, ctx, st);
     mark(kPrep, false, st);
@@ -331,6 +306,71 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
         ops->verify_root(v, layer, st);
         mark(kRoot, false, st);
     }
+}
+
+void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_sm,
+                    const uint64_t* d_sm_off, const uint64_t* d_smlen, const uint8_t* d_pk, uint32_t npk,
+                    const uint32_t* d_pk_index, int* d_status, cudaStream_t st)
+{
+    XB_CUDA(cudaMemsetAsync(work_, 0, 3 * sizeof(unsigned long long), st));
+    if (!count) return;
+    const uint32_t n = p.n, len = ops->len, nh = len - 1 + p.tree_height;
+    void* ctx = s_ctx_.get((size_t)npk * ops->ctx_bytes);
+    ops->make_ctx(d_pk + n, 2 * n, nullptr, 0, nullptr, 0, npk, ctx, st);
+    VerifyArgs v;
+    v.sm = d_sm;
+    v.sm_off = d_sm_off;
+    v.smlen = d_smlen;
+    v.key = d_pk_index;
+    v.key_root = d_pk;
+    v.key_stride = 2 * n;
+    v.node = s_node_.as<uint8_t>((size_t)count * n);
+    v.lens = s_lens_.as<uint8_t>((size_t)count * len);
+    v.idx = s_idx_.as<uint64_t>(count);
+    v.status = d_status;
+    v.wpk = s_wpk_.as<uint8_t>((size_t)count * len * n);
+    v.wpk2 = s_wpk2_.as<uint8_t>((size_t)count * ((len + 1) / 2) * n);
+    v.leaf = s_leaf_.as<uint8_t>((size_t)count * n);
+    v.refs = s_refs_.as<LeafRef>(count);
+    v.hpre = s_hpre_.get((size_t)count * p.d * nh * ops->hpre_bytes);
+    uint32_t* hist = s_hist_.as<uint32_t>(2 * 32 * p.d + 2);  // two groups + 2 group sizes
+    uint32_t* list = s_list_.as<uint32_t>((size_t)count * len + 2 * (size_t)count);
+    v.hist = hist;
+    v.list = list;
+    v.sel = nullptr;
+    v.sel_n = nullptr;
+    v.work = work_;
+    v.count = count;
+    v.index_bytes = p.index_bytes;
+    v.sig_bytes = p.sig_bytes;
+    v.tree_height = p.tree_height;
+    v.d = p.d;
+    XB_CUDA(cudaMemsetAsync(hist, 0, (2 * 32 * p.d + 2) * sizeof(uint32_t), st));
+    // Large batches run as two groups on two streams: signatures whose
+    // H_msg is short start their chains at once while the long messages are
+    // still being hashed (H_msg is a serial chain of compressions).  The
+    // profiling pass keeps one sequence so each kernel's time is its own.
+    if (count < kSplitMin || profiling) {
+        verify_sequence(ops, p, v, ctx, st);
+        return;
+    }
+    uint32_t* n2 = hist + 2 * 32 * p.d;
+    uint32_t* sel_short = list + (size_t)count * len;
+    uint32_t* sel_long = sel_short + count;
+    ops->verify_partition(v, kShortHmsgBlocks, sel_short, sel_long, n2, st);
+    VerifyArgs a = v, b = v;
+    a.sel = sel_short;
+    a.sel_n = n2;
+    b.sel = sel_long;
+    b.sel_n = n2 + 1;
+    b.hist = hist + 32 * p.d;
+    b.list = s_list2_.as<uint32_t>((size_t)count * len);  // each group has its own chain list
+    XB_CUDA(cudaEventRecord(fork_, st));
+    XB_CUDA(cudaStreamWaitEvent(aux_, fork_, 0));
+    verify_sequence(ops, p, b, ctx, aux_);
+    verify_sequence(ops, p, a, ctx, st);
+    XB_CUDA(cudaEventRecord(join_, aux_));
+    XB_CUDA(cudaStreamWaitEvent(st, join_, 0));
 }
 
 void Engine::last_verify_work(unsigned long long out[3])

@@ -18,6 +18,7 @@ namespace xb {
 
 struct LeafRef;
 struct TreeJob;
+struct VerifyArgs;
 
 class CudaFailure : public std::runtime_error {
    public:
@@ -113,6 +114,15 @@ class Engine {
     void core_hash(const FamilyOps* ops, uint32_t count, const uint8_t* d_in, const uint64_t* d_off,
                    const uint64_t* d_len, uint8_t* d_out, cudaStream_t st);
 
+    // Verify launch sequence over the signatures v selects (all when
+    // v.sel is null), on one stream.
+    void verify_sequence(const FamilyOps* ops, const xmss_params& p, const VerifyArgs& v, const void* ctx,
+                         cudaStream_t st);
+    // Batches of at least kSplitMin signatures are verified as two groups
+    // split at kShortHmsgBlocks hash blocks of H_msg.
+    static constexpr uint32_t kSplitMin = 1024;
+    static constexpr uint32_t kShortHmsgBlocks = 16;
+
     // Work counters of the last verify (see xmss_b200_last_verify_work).
     void last_verify_work(unsigned long long out[3]);
 
@@ -130,10 +140,12 @@ class Engine {
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
     cudaEvent_t done_ = nullptr;
+    cudaStream_t aux_ = nullptr;  // second stream of split verify batches
+    cudaEvent_t fork_ = nullptr, join_ = nullptr;
     bool have_done_ = false;
     // pipeline scratch
     DevBuf s_ctx_, s_jobs_, s_refs_, s_wpk_, s_wpk2_, s_nodes_, s_keys_, s_node_, s_lens_, s_idx_, s_leaf_,
-        s_work_, s_tree_off_, s_key_idx_, s_mlen_, s_hpre_, s_hist_, s_list_;
+        s_work_, s_tree_off_, s_key_idx_, s_mlen_, s_hpre_, s_hist_, s_list_, s_list2_;
     PinnedBuf h_jobs_;
     unsigned long long* work_ = nullptr;
     struct Mark {

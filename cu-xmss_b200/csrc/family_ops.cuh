@@ -52,6 +52,12 @@ struct Launch {
         if (!items) return;
         k_tree_level<F><<<grid_for(items), kBlock, 0, st>>>(jobs, njobs, h, level, nodes, (const Ctx*)ctx);
     }
+    static void verify_partition(const VerifyArgs& v, uint32_t blocks_max, uint32_t* sel_short, uint32_t* sel_long,
+                                 uint32_t* n2, cudaStream_t st)
+    {
+        if (!v.count) return;
+        k_verify_partition<F><<<grid_for(v.count), kBlock, 0, st>>>(v, blocks_max, sel_short, sel_long, n2);
+    }
     static void verify_prep(const VerifyArgs& v, const void* ctx, cudaStream_t st)
     {
         if (!v.count) return;
@@ -116,6 +122,7 @@ struct Launch {
         o.ltree_level = ltree_level;
         o.tree_level = tree_level;
         o.hpre_bytes = sizeof(typename F::HPre);
+        o.verify_partition = verify_partition;
         o.verify_prep = verify_prep;
         o.verify_scatter = verify_scatter;
         o.verify_chains = verify_chains;

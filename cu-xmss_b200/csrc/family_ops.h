@@ -28,6 +28,8 @@ struct FamilyOps {
     void (*tree_level)(const TreeJob* jobs, uint32_t njobs, int h, int level, uint8_t* nodes, const void* ctx,
                        cudaStream_t st);
     size_t hpre_bytes;  // sizeof(F::HPre)
+    void (*verify_partition)(const VerifyArgs& v, uint32_t blocks_max, uint32_t* sel_short, uint32_t* sel_long,
+                             uint32_t* n2, cudaStream_t st);
     void (*verify_prep)(const VerifyArgs& v, const void* ctx, cudaStream_t st);
     void (*verify_scatter)(const VerifyArgs& v, uint32_t layer, cudaStream_t st);
     void (*verify_chains)(const VerifyArgs& v, uint32_t layer, const void* ctx, cudaStream_t st);

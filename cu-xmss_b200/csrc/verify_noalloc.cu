@@ -146,6 +146,8 @@ extern "C" int xmss_b200_sign_open_device_noalloc(uint32_t oid, int mt, uint32_t
     v.hpre = base + o_hpre;
     v.hist = (uint32_t*)(base + o_hist);
     v.list = (uint32_t*)(base + o_list);
+    v.sel = nullptr;
+    v.sel_n = nullptr;
     v.work = nullptr;
     v.count = count;
     v.index_bytes = p.index_bytes;

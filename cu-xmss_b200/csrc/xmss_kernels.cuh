@@ -251,6 +251,8 @@ struct VerifyArgs {
     void* hpre;               // [count][d][NH] F::HPre, NH = LEN - 1 + tree_height
     uint32_t* hist;           // [d][32]: chains per step count, then bucket cursors
     uint32_t* list;           // [count * LEN] chain work list, longest first
+    const uint32_t* sel;      // optional: the signatures this launch sequence handles
+    const uint32_t* sel_n;    // (device) number of entries in sel; sel == null: all
     unsigned long long* work; // [3] H_msg blocks, F calls, H calls (accumulated)
     uint32_t count;
     uint32_t index_bytes;
@@ -289,6 +291,10 @@ __device__ __forceinline__ void flush_hist(uint32_t* sh_hist, uint32_t* hist)
     if (threadIdx.x < 16 && sh_hist[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh_hist[threadIdx.x]);
 }
 
+// Signatures handled by this launch sequence: all of them, or the selection.
+__device__ __forceinline__ uint32_t sel_count(const VerifyArgs& v) { return v.sel ? *v.sel_n : v.count; }
+__device__ __forceinline__ uint32_t sel_sig(const VerifyArgs& v, uint32_t i) { return v.sel ? v.sel[i] : i; }
+
 template <class F>
 __device__ __forceinline__ void layer_addr(uint64_t idx, uint32_t th, uint32_t layer, uint32_t& leaf, uint64_t& tree)
 {
@@ -309,8 +315,9 @@ __global__ void __launch_bounds__(64) k_verify_prep(VerifyArgs v, uint32_t hmsg_
     if (blockIdx.x < hmsg_blocks_n) {
         if (threadIdx.x < 16) sh_hist[threadIdx.x] = 0;
         __syncthreads();
-        const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-        if (s < v.count) {
+        const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i < sel_count(v)) {
+            const uint32_t s = sel_sig(v, i);
             const uint64_t smlen = v.smlen[s];
             if (smlen < v.sig_bytes) {  // the reference would underflow here; reject
                 v.status[s] = -1;
@@ -338,10 +345,12 @@ __global__ void __launch_bounds__(64) k_verify_prep(VerifyArgs v, uint32_t hmsg_
         return;
     }
     const uint32_t nh = F::LEN - 1 + v.tree_height;
-    const uint64_t item = (uint64_t)(blockIdx.x - hmsg_blocks_n) * blockDim.x + threadIdx.x;
-    if (item >= (uint64_t)v.count * v.d * nh) return;
-    const uint32_t s = (uint32_t)(item / ((uint64_t)v.d * nh));
-    const uint32_t rem = (uint32_t)(item - (uint64_t)s * v.d * nh);
+    const uint64_t pitem = (uint64_t)(blockIdx.x - hmsg_blocks_n) * blockDim.x + threadIdx.x;
+    if (pitem >= (uint64_t)sel_count(v) * v.d * nh) return;
+    const uint32_t si = (uint32_t)(pitem / ((uint64_t)v.d * nh));
+    const uint32_t rem = (uint32_t)(pitem - (uint64_t)si * v.d * nh);
+    const uint32_t s = sel_sig(v, si);
+    const uint64_t item = (uint64_t)s * v.d * nh + rem;
     const uint32_t layer = rem / nh;
     uint32_t node = rem - layer * nh;
     if (v.smlen[s] < v.sig_bytes) return;
@@ -368,6 +377,24 @@ __global__ void __launch_bounds__(64) k_verify_prep(VerifyArgs v, uint32_t hmsg_
     ((HPre*)v.hpre)[item] = hp;
 }
 
+// Splits the signatures into a short-H_msg group (at most `blocks_max` hash
+// blocks) and a long one, so the long messages' serial H_msg runs on its own
+// stream while the short group's chains keep the GPU busy.
+template <class F>
+__global__ void k_verify_partition(VerifyArgs v, uint32_t blocks_max, uint32_t* sel_short, uint32_t* sel_long,
+                                   uint32_t* n2)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.count) return;
+    const uint64_t smlen = v.smlen[s];
+    const bool lng = smlen >= v.sig_bytes && hmsg_blocks<F>(smlen - v.sig_bytes) > blocks_max;
+    if (lng) {
+        sel_long[atomicAdd(&n2[1], 1u)] = s;
+    } else {
+        sel_short[atomicAdd(&n2[0], 1u)] = s;
+    }
+}
+
 // Buckets the chains of one layer by step count (longest first) into
 // v.list; zero-step chains are copied straight to the WOTS pk.  Also writes
 // the L-tree address of every signature.
@@ -378,10 +405,12 @@ __global__ void __launch_bounds__(256) k_verify_scatter(VerifyArgs v, uint32_t l
     uint32_t* hist = v.hist + 32 * layer;
     if (threadIdx.x < 16) sh_cnt[threadIdx.x] = 0;
     __syncthreads();
-    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool in = item < (uint64_t)v.count * F::LEN;
-    const uint32_t s = in ? (uint32_t)(item / F::LEN) : 0;
-    const uint32_t chain = in ? (uint32_t)(item - (uint64_t)s * F::LEN) : 0;
+    const uint64_t it = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = it < (uint64_t)sel_count(v) * F::LEN;
+    const uint32_t si = in ? (uint32_t)(it / F::LEN) : 0;
+    const uint32_t chain = in ? (uint32_t)(it - (uint64_t)si * F::LEN) : 0;
+    const uint32_t s = in ? sel_sig(v, si) : 0;
+    const uint64_t item = (uint64_t)s * F::LEN + chain;
     const bool live = in && v.status[s] == 0;
     uint32_t steps = 0, local = 0;
     if (live) {
@@ -456,9 +485,10 @@ __global__ void __launch_bounds__(128) k_verify_ltree(VerifyArgs v, uint32_t lay
     using HPre = typename F::HPre;
     const int pairs = (cnt_in + 1) >> 1;
     const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (item >= (uint64_t)v.count * pairs) return;
-    const uint32_t s = (uint32_t)(item / pairs);
-    const int p = (int)(item - (uint64_t)s * pairs);
+    if (item >= (uint64_t)sel_count(v) * pairs) return;
+    const uint32_t si = (uint32_t)(item / pairs);
+    const int p = (int)(item - (uint64_t)si * pairs);
+    const uint32_t s = sel_sig(v, si);
     if (v.status[s] != 0) return;
     const uint8_t* sp = src + ((uint64_t)s * src_stride) * F::N;
     uint8_t* out = (cnt_in == 2) ? v.leaf + (uint64_t)s * F::N : dst + ((uint64_t)s * dst_stride + p) * F::N;
@@ -485,8 +515,9 @@ __global__ void __launch_bounds__(64) k_verify_root(VerifyArgs v, uint32_t layer
     __shared__ uint32_t sh_hist[16];
     if (threadIdx.x < 16) sh_hist[threadIdx.x] = 0;
     __syncthreads();
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < v.count && v.status[s] == 0) {
+    const uint32_t si = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t s = si < sel_count(v) ? sel_sig(v, si) : 0;
+    if (si < sel_count(v) && v.status[s] == 0) {
         const uint32_t th = v.tree_height;
         uint32_t leafidx;
         uint64_t tree;

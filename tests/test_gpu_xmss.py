@@ -196,3 +196,35 @@ def test_sign_batch_long_messages_match_oracle(xb, oracle):
     buf, off, ln = xb.pack(sms, align=16)
     st = xb.sign_open_batch(False, buf, off, ln, pks, keyix.astype(np.uint32))
     assert (st == 0).all()
+
+
+def test_large_batch_two_group_path(xb, oracle):
+    """Batches of 1024+ signatures are verified as a short-H_msg and a
+    long-H_msg group on two streams; the accept bitmap must still be exact
+    (corruptions anywhere, the last-index quirk) and agree with the oracle."""
+    rng = np.random.default_rng(41)
+    p, po = xb.parse_oid(1), oracle.params(1)
+    count, keys = 1100, 4
+    seeds = np.frombuffer(rng.bytes(keys * 96), np.uint8).reshape(keys, 96)
+    pks, sks = xb.keypair_batch(1, False, seeds)
+    keyix = rng.integers(0, keys, count).astype(np.uint32)
+    idx = rng.integers(0, 1024, count)
+    idx[:3] = 1023
+    mlen = np.exp(rng.uniform(np.log(1), np.log(4096), count)).astype(int)
+    msgs = [rng.bytes(int(L)) for L in mlen]
+    rows = np.array(sks[keyix])
+    for i in range(count):
+        rows[i, 4:8] = np.frombuffer(int(idx[i]).to_bytes(4, "big"), np.uint8)
+    ret, sms = xb.sign_batch(False, rows, msgs)
+    assert (ret == 0).all()
+    expect = np.where(idx == 1023, -1, 0)
+    sms = [bytearray(s) for s in sms]
+    for i in range(5, count, 9):
+        sms[i][int(rng.integers(0, len(sms[i])))] ^= 1 << int(rng.integers(0, 8))
+        expect[i] = -1
+    sms = [bytes(s) for s in sms]
+    buf, off, ln = xb.pack(sms, align=8)
+    st = xb.sign_open_batch(False, buf, off, ln, pks, keyix)
+    assert (st == expect).all()
+    for i in rng.choice(count, 40, replace=False):
+        assert oracle.sign_open(po, sms[i], bytes(pks[keyix[i], 4:]))[0] == st[i]
