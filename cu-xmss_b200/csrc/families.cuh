@@ -411,35 +411,68 @@ struct Sha256N32T : FamBase<32, 32, true> {
         for (int i = 0; i < 8; i++) x[i] = t[i];
     }
 
+    // thash_h runs as one loop over its six compressions around a single
+    // compression body: the tree kernels that call it are throughput bound,
+    // and separately inlined bodies overflow the instruction cache.
+    // thash_h in one loop with the masks folded into the inputs as soon as
+    // they exist: 0 mask PRF (km 1) -> l ^= m1, 1 mask PRF (km 2) -> r ^= m2,
+    // 2 key PRF (km 0), 3 toByte(1,32) || key, 4 l || r, 5 padding.
+    // o may alias l or r.
     __device__ static void thash_h(uint32_t (&o)[8], const uint32_t (&l)[8], const uint32_t (&r)[8],
                                    const Ctx& c, uint32_t (&a)[8])
     {
-        uint32_t t[8], st[8], w[16];
-        a[7] = 0;
-        prf_adrs(t, c, a);  // key
+        uint32_t lc[8], rc[8], t[8];
 #pragma unroll
-        for (int i = 0; i < 7; i++) w[i] = 0;
-        w[7] = 1;
+        for (int i = 0; i < 8; i++) {
+            lc[i] = l[i];
+            rc[i] = r[i];
+        }
+#pragma unroll 1
+        for (uint32_t k = 0; k < 6; k++) {
+            uint32_t st[8], w[16];
+            if (k <= 2) {
 #pragma unroll
-        for (int i = 0; i < 8; i++) w[8 + i] = t[i];
-        sha256_iv(st);
-        compress(st, w);
-        a[7] = 1;
-        prf_adrs(t, c, a);
+                for (int i = 0; i < 7; i++) w[i] = a[i];
+                w[7] = (k == 2) ? 0u : k + 1;
+                w[8] = 0x80000000u;
 #pragma unroll
-        for (int i = 0; i < 8; i++) w[i] = l[i] ^ t[i];
-        a[7] = 2;
-        prf_adrs(t, c, a);
+                for (int i = 9; i < 15; i++) w[i] = 0;
+                w[15] = 768;
 #pragma unroll
-        for (int i = 0; i < 8; i++) w[8 + i] = r[i] ^ t[i];
-        compress(st, w);
-        w[0] = 0x80000000u;
+                for (int i = 0; i < 8; i++) st[i] = c.prf_mid[i];
+            } else if (k == 3) {
 #pragma unroll
-        for (int i = 1; i < 15; i++) w[i] = 0;
-        w[15] = 1024;
-        compress(st, w);
+                for (int i = 0; i < 7; i++) w[i] = 0;
+                w[7] = 1;
 #pragma unroll
-        for (int i = 0; i < 8; i++) o[i] = st[i];
+                for (int i = 0; i < 8; i++) w[8 + i] = t[i];
+                sha256_iv(st);
+            } else if (k == 4) {
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    w[i] = lc[i];
+                    w[8 + i] = rc[i];
+                    st[i] = t[i];
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 8; i++) st[i] = t[i];
+                w[0] = 0x80000000u;
+#pragma unroll
+                for (int i = 1; i < 15; i++) w[i] = 0;
+                w[15] = 1024;
+            }
+            compress(st, w);
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                if (k == 0) lc[i] ^= st[i];
+                else if (k == 1) rc[i] ^= st[i];
+                else t[i] = st[i];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) o[i] = t[i];
+        a[7] = 2;  // as set_key_and_mask leaves it (hash.c:146-147)
     }
 
     __device__ static void h_pre(HPre& o, const Ctx& c, uint32_t (&a)[8])
@@ -975,10 +1008,13 @@ __device__ __forceinline__ void load_block64_be(uint32_t (&w)[16], const uint8_t
 }
 
 // H_msg for SHA-256 with n = 32: the 128-byte prefix is exactly two blocks,
-// so M starts block aligned.  Full message blocks are loaded one block ahead
-// of the compression that consumes them.
-__device__ __forceinline__ void hmsg_sha256_n32(uint32_t (&out)[8], const uint32_t (&R)[8], const uint32_t (&root)[8],
-                                                uint64_t idx, const uint8_t* m, uint64_t mlen)
+// so M starts block aligned; full message blocks are loaded one block ahead
+// of the compression that consumes them.  H_msg is a serial chain, so the
+// prefix, body and tail compressions are written out (a single-body loop
+// measured slower here: its per-block setup lengthens the chain).
+__device__ __forceinline__ void hmsg_sha256_n32(uint32_t (&out)[8], const uint32_t (&R)[8],
+                                                       const uint32_t (&root)[8], uint64_t idx, const uint8_t* m,
+                                                       uint64_t mlen)
 {
     uint32_t st[8], w[16];
     sha256_iv(st);
@@ -1004,14 +1040,13 @@ __device__ __forceinline__ void hmsg_sha256_n32(uint32_t (&out)[8], const uint32
         if (b + 1 < nfull) load_block64_be(nxt, m, mlen, 64 * (b + 1));
         sha256_compress(st, w);
     }
-    // tail: remaining bytes, 0x80, zero fill, 64-bit bit length of 128 + mlen
     const uint64_t L = 128 + mlen;
     const uint64_t o0 = 64 * nfull;
     const int tail_blocks = ((mlen - o0) + 9 > 64) ? 2 : 1;
     for (int b = 0; b < tail_blocks; b++) {
 #pragma unroll
         for (int j = 0; j < 16; j++) {
-            const uint64_t o = o0 + 64 * b + 4 * j;  // offset into M
+            const uint64_t o = o0 + 64 * b + 4 * j;
             uint32_t le = (o < mlen) ? fetch4_le(m, mlen, o) : 0;
             if (o <= mlen && mlen < o + 4) le |= 0x80u << (8 * (mlen - o));
             w[j] = bswap32(le);
