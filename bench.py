@@ -143,6 +143,27 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
+# replicas: every rank verifies its own batch, no data-path collective
+# ---------------------------------------------------------------------------
+
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The slowest rank's time (all ranks get it)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(per_rank_items: int, world: int, steps: int, seconds: float) -> float:
+    """Whole-job throughput of `world` replicas (weak scaling)."""
+    return per_rank_items * world * steps / seconds
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 
@@ -203,12 +224,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if world > 1:
         dist.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    t_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([t_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
-    value = NUM_SIGS * world * args.steps / (t_ms / 1e3)
+    t_ms = max_over_ranks(float(sum(step_ms)), world, dev)
+    value = replica_rate(NUM_SIGS, world, args.steps, t_ms / 1e3)
 
     # ---- per-kernel timing (separate pass; profiling serialises calls) ----
     xb.profile(True)
@@ -236,6 +253,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         torch.cuda.synchronize()
         probe[kind] = probe_blocks * 128 * iters / (pe0.elapsed_time(pe1) / 1e3)
     probe_rate = max(probe.values())
+    # latency of one dependent compression for a lone warp per SM (what the
+    # serial phases, H_msg and the tree levels, are bound by)
+    lat_iters = 500
+    xb.rate_probe(20, 148, 10, sink.data_ptr(), sh)
+    pe0.record(stream)
+    xb.rate_probe(20, 148, lat_iters, sink.data_ptr(), sh)
+    pe1.record(stream)
+    torch.cuda.synchronize()
+    lone_us = pe0.elapsed_time(pe1) * 1e3 / lat_iters
 
     # ---- e2e through the host-buffer C-ABI ----
     h_sm = torch.from_numpy(w["buf"]).pin_memory().numpy()
@@ -254,12 +280,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         st = xb.sign_open_batch(False, h_sm, h_off, h_len, h_pk, h_kix)
         e2e_t.append(time.perf_counter() - t0)
     correct = correct and bool((st == w["expect"]).all())
-    e2e_s = float(sum(e2e_t))
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = NUM_SIGS * world * args.steps / e2e_s
+    e2e_s = max_over_ranks(float(sum(e2e_t)), world, dev)
+    e2e_value = replica_rate(NUM_SIGS, world, args.steps, e2e_s)
     h2d = int(w["buf"].nbytes + h_off.nbytes + h_len.nbytes + NUM_KEYS * 2 * n + h_kix.nbytes)
     d2h = 4 * NUM_SIGS
 
@@ -308,6 +330,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                                     f"{iters} SHA-256 compressions (same core as the kernels), best of the "
                                     "ALU-pipe and FMA-pipe forms",
                      "probe_gcompr_s": {"alu_form": probe[10] / 1e9, "fma_form": probe[11] / 1e9},
+                     "lone_warp_us_per_compression": lone_us,
                      "work_per_launch": {"compressions": comp_chain, "f_calls": work.f_calls},
                      "phase_ms": med,
                      "pipeline_gcompr_s": pipeline_rate,
@@ -324,26 +347,35 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
 
 def keygen_rate(xb, torch, dev, sh):
-    """XMSS-SHA2_16_256 keygen of 8 seeded keys: leaves/s and compressions/s."""
-    oid = 0x02
-    p = xb.parse_oid(oid)
-    count = 8
+    """Batched keygen of the survey's config 3: 8 XMSS-SHA2_16_256 keys and
+    1 XMSS-SHA2_20_256 key from seeded seeds, in one timed region."""
     rng = np.random.default_rng(SEED + 16)
-    seeds = torch.from_numpy(np.frombuffer(rng.bytes(count * 3 * p.n), np.uint8).copy()).to(dev)
-    d_pk = torch.empty(count * 2 * p.n, dtype=torch.uint8, device=dev)
-    d_sk = torch.empty(count * p.sk_bytes, dtype=torch.uint8, device=dev)
-    xb.keypair_device(oid, False, count, seeds.data_ptr(), d_pk.data_ptr(), d_sk.data_ptr(), sh)
+    jobs = []
+    for oid, count in ((0x02, 8), (0x03, 1)):
+        p = xb.parse_oid(oid)
+        seeds = torch.from_numpy(np.frombuffer(rng.bytes(count * 3 * p.n), np.uint8).copy()).to(dev)
+        d_pk = torch.empty(count * 2 * p.n, dtype=torch.uint8, device=dev)
+        d_sk = torch.empty(count * p.sk_bytes, dtype=torch.uint8, device=dev)
+        jobs.append((oid, count, p, seeds, d_pk, d_sk))
+
+    def run():
+        for oid, count, p, seeds, d_pk, d_sk in jobs:
+            xb.keypair_device(oid, False, count, seeds.data_ptr(), d_pk.data_ptr(), d_sk.data_ptr(), sh)
+
+    run()  # warm-up (scratch growth)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    xb.keypair_device(oid, False, count, seeds.data_ptr(), d_pk.data_ptr(), d_sk.data_ptr(), sh)
+    run()
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    leaves = count << p.full_height
-    comp = count * (((1 << 16) * (67 * 2 + 67 * 15 * 4 + 66 * 6)) + 6 * ((1 << 16) - 1))
-    return {"metric": "XMSS-SHA2_16_256 keygen leaves/s (8 keys x 65,536 leaves)", "value": leaves / (ms / 1e3),
-            "unit": "leaves/s", "ms": ms, "gcompr_s": comp / (ms / 1e3) / 1e9, "compressions": comp}
+    leaves = sum(count << p.full_height for _, count, p, *_ in jobs)
+    leaf_compr = 67 * 2 + 67 * 15 * 4 + 66 * 6  # PRF_keygen, 15 F per chain, L-tree
+    comp = sum(count * ((leaf_compr << p.full_height) + 6 * ((1 << p.full_height) - 1)) for _, count, p, *_ in jobs)
+    return {"metric": "keygen leaves/s: 8 x XMSS-SHA2_16_256 + 1 x XMSS-SHA2_20_256 (1,572,864 leaves)",
+            "value": leaves / (ms / 1e3), "unit": "leaves/s", "ms": ms, "gcompr_s": comp / (ms / 1e3) / 1e9,
+            "compressions": comp}
 
 
 def read_traffic():
@@ -519,12 +551,95 @@ def make_workload_cpu(count: int = 512, keys: int = 8):
 
 # ---------------------------------------------------------------------------
 
+MIX_SETS = (("XMSSMT-SHA2_20/2_256", 0x01, True), ("XMSSMT-SHA2_40/4_256", 0x04, True),
+            ("XMSS-SHA2_10_512", 0x04, False), ("XMSS-SHAKE_10_256", 0x07, False))
+
+
+def run_mix(args):
+    """Config 4: per parameter set one seeded key, 2,048 signatures at
+    consecutive indices over messages log-uniform in 32 B..64 KB (batched
+    sign through the host C-ABI), then a batched verify of all of them."""
+    import torch
+
+    import xmss_b200 as xb
+
+    xb.init(0)
+    rng = np.random.default_rng(SEED + 4)
+    out = {"workload": "mix", "sets": []}
+    for name, oid, mt in MIX_SETS:
+        p = xb.parse_oid(oid, mt)
+        count = 2048
+        # consecutive indices per key; a key of height 10 has 1,023 usable ones
+        cap = min((1 << p.full_height) - 1, count)
+        nkeys = -(-count // cap)
+        seeds = np.frombuffer(rng.bytes(nkeys * 3 * p.n), np.uint8).reshape(nkeys, -1)
+        pks, sks = xb.keypair_batch(oid, mt, seeds)
+        start = 0 if cap < count else int(rng.integers(0, (1 << min(p.full_height, 40)) - count))
+        mlen = np.exp(rng.uniform(np.log(32), np.log(65536), count)).astype(np.int64)
+        msgs = [rng.bytes(int(L)) for L in mlen]
+        kix = (np.arange(count) // cap).astype(np.uint32)
+        rows = np.array(sks[kix])
+        for i in range(count):
+            rows[i, 4:4 + p.index_bytes] = np.frombuffer((start + i % cap).to_bytes(p.index_bytes, "big"),
+                                                         np.uint8)
+        xb.sign_batch(mt, rows.copy()[:64], msgs[:64])  # warm-up
+        t0 = time.perf_counter()
+        ret, sms = xb.sign_batch(mt, rows, msgs)
+        t_sign = time.perf_counter() - t0
+        buf, off, ln = xb.pack(sms, align=16)
+        xb.sign_open_batch(mt, buf, off, ln, pks, kix)  # warm-up
+        t0 = time.perf_counter()
+        st = xb.sign_open_batch(mt, buf, off, ln, pks, kix)
+        t_ver = time.perf_counter() - t0
+        w = xb.last_verify_work()
+        out["sets"].append({"set": name, "keys": nkeys, "signs": count, "signs_per_s": count / t_sign,
+                            "verifies_per_s": count / t_ver, "sign_s": t_sign, "verify_s": t_ver,
+                            "mean_mlen": float(mlen.mean()), "all_signed": bool((ret == 0).all()),
+                            "all_verified": bool((st == 0).all()),
+                            "verify_work": {"hmsg_blocks": w.hmsg_blocks, "f_calls": w.f_calls,
+                                            "h_calls": w.h_calls}})
+        log(out["sets"][-1])
+    return out
+
+
+def run_plain(args):
+    """Config 1 and the per-call baseline: XMSS-SHA2_10_256 keypair from a
+    seeded seed, then 16 x (xmss_sign, xmss_sign_open) of 32-byte messages,
+    one reference-API call at a time (each sign recomputes its subtree)."""
+    import xmss_b200 as xb
+
+    xb.init(0)
+    rng = np.random.default_rng(SEED + 1)
+    p = xb.parse_oid(1)
+    seed = rng.bytes(96)
+    t0 = time.perf_counter()
+    r, pk, sk = xb.xmssmt_core_seed_keypair(p, seed)
+    t_kp = time.perf_counter() - t0
+    pkf, skf = b"\0\0\0\x01" + pk, b"\0\0\0\x01" + sk
+    xb.xmss_sign(skf, b"w" * 32)
+    ts, tv = [], []
+    for i in range(16):
+        m = rng.bytes(32)
+        t0 = time.perf_counter()
+        r, skf, sm = xb.xmss_sign(skf, m)
+        ts.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        rv, mo = xb.xmss_sign_open(sm, pkf)
+        tv.append(time.perf_counter() - t0)
+        assert r == 0 and rv == 0 and mo == m
+    return {"workload": "plain", "keypair_ms": 1e3 * t_kp, "sign_ms_median": 1e3 * float(np.median(ts)),
+            "verify_ms_median": 1e3 * float(np.median(tv)), "signs_per_s": 1 / float(np.median(ts)),
+            "verifies_per_s": 1 / float(np.median(tv))}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["verify", "mix", "plain"], default="verify",
+                    help="verify: the headline line; mix / plain: the XMSS^MT + wide-hash and per-call configs")
     ap.add_argument("--skip-keygen", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=2.5)
@@ -546,6 +661,10 @@ def main():
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     if args.impl == "reference":
         out = run_reference(args, rank, world)
+    elif args.workload == "mix":
+        out = run_mix(args)
+    elif args.workload == "plain":
+        out = run_plain(args)
     else:
         out = run_ours(args, rank, world, local_rank)
     if out is not None:
