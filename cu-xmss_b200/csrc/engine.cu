@@ -28,27 +28,56 @@ void* DevBuf::get(size_t bytes)
     if (bytes > cap_) {
         size_t cap = std::max(bytes, cap_ + cap_ / 2);
         cap = (cap + 4095) & ~(size_t)4095;
-        if (p_) {
-            XB_CUDA(cudaDeviceSynchronize());
-            XB_CUDA(cudaFree(p_));
+        if (ordered_) {
+            // stream-ordered: work already queued on order_ keeps the old
+            // block until it has run; nothing else waits
+            if (p_) XB_CUDA(cudaFreeAsync(p_, order_));
             p_ = nullptr;
             cap_ = 0;
+            XB_CUDA(cudaMallocAsync(&p_, cap, order_));
+        } else {
+            if (p_) {
+                XB_CUDA(cudaDeviceSynchronize());
+                XB_CUDA(cudaFree(p_));
+                p_ = nullptr;
+                cap_ = 0;
+            }
+            XB_CUDA(cudaMalloc(&p_, cap));
         }
-        XB_CUDA(cudaMalloc(&p_, cap));
         cap_ = cap;
     }
     return p_;
 }
 
+void Workspace::order_on(cudaStream_t st)
+{
+    for (DevBuf* b : {&ctx, &jobs, &refs, &wpk, &wpk2, &nodes, &keys, &node, &lens, &idx, &leaf, &hpre, &hist, &list,
+                      &list2, &aux, &work})
+        b->order_on(st);
+}
+
 PinnedBuf::~PinnedBuf()
 {
     if (p_) cudaFreeHost(p_);
+    for (void* q : retired_) cudaFreeHost(q);
 }
 
 void* PinnedBuf::get(size_t bytes)
 {
     if (bytes == 0) bytes = 1;
     if (bytes > cap_) {
+        if (keep_old_) {
+            // the owner guarantees no copy uses the old block when it grows;
+            // it is kept (not freed: cudaFreeHost may wait for the device)
+            size_t cap = std::max(bytes, 2 * cap_);
+            cap = (cap + 4095) & ~(size_t)4095;
+            if (p_) retired_.push_back(p_);
+            p_ = nullptr;
+            cap_ = 0;
+            XB_CUDA(cudaMallocHost(&p_, cap));
+            cap_ = cap;
+            return p_;
+        }
         size_t cap = std::max(bytes, cap_ + cap_ / 2);
         cap = (cap + 4095) & ~(size_t)4095;
         if (p_) {
@@ -153,9 +182,9 @@ cudaEvent_t Engine::event()
     return e;
 }
 
-void Engine::mark(int phase, bool start, cudaStream_t st)
+void Engine::mark(int phase, bool start, cudaStream_t st, bool on)
 {
-    if (!profiling) return;
+    if (!profiling || !on) return;
     if (start) {
         marks_.push_back(Mark{phase, event(), nullptr});
         XB_CUDA(cudaEventRecord(marks_.back().a, st));
@@ -232,42 +261,43 @@ static void run_ltree(const FamilyOps* ops, const LeafRef* refs, uint32_t nslots
 }
 
 void Engine::build_trees(const FamilyOps* ops, const TreeJob* d_jobs, uint32_t njobs, int h, uint8_t* d_nodes,
-                         const void* d_ctx, cudaStream_t st)
+                         const void* d_ctx, cudaStream_t st, Workspace& w)
 {
+    const bool on = &w == &ws_;  // server workspaces record no marks
     const uint64_t total = (uint64_t)njobs << h;
     const uint64_t per_slot = (uint64_t)ops->len * ops->n;
     const uint64_t cap = std::max<uint64_t>(1, std::min<uint64_t>(total, kChainScratchBytes / per_slot));
-    uint8_t* wpk = s_wpk_.as<uint8_t>(cap * per_slot);
-    uint8_t* wpk2 = s_wpk2_.as<uint8_t>(cap * ((ops->len + 1) / 2) * ops->n);
-    LeafRef* refs = s_refs_.as<LeafRef>(cap);
+    uint8_t* wpk = w.wpk.as<uint8_t>(cap * per_slot);
+    uint8_t* wpk2 = w.wpk2.as<uint8_t>(cap * ((ops->len + 1) / 2) * ops->n);
+    LeafRef* refs = w.refs.as<LeafRef>(cap);
     for (uint64_t s0 = 0; s0 < total; s0 += cap) {
         const uint64_t ns = std::min(cap, total - s0);
-        mark(kChains, true, st);
+        mark(kChains, true, st, on);
         ops->keygen_chains(d_jobs, h, s0, ns, d_ctx, wpk, refs, st);
-        mark(kChains, false, st);
-        mark(kLtree, true, st);
+        mark(kChains, false, st, on);
+        mark(kLtree, true, st, on);
         run_ltree(ops, refs, (uint32_t)ns, wpk, wpk2, d_nodes, d_ctx, nullptr, st);
-        mark(kLtree, false, st);
+        mark(kLtree, false, st, on);
     }
-    mark(kTree, true, st);
+    mark(kTree, true, st, on);
     for (int level = 0; level < h; level++) ops->tree_level(d_jobs, njobs, h, level, d_nodes, d_ctx, st);
-    mark(kTree, false, st);
+    mark(kTree, false, st, on);
 }
 
 void Engine::keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_seeds,
-                     uint8_t* d_pk, uint8_t* d_sk, cudaStream_t st)
+                     uint8_t* d_pk, uint8_t* d_sk, cudaStream_t st, Workspace& w)
 {
     if (!count) return;
     const uint32_t n = p.n, th = p.tree_height;
-    void* ctx = s_ctx_.get((size_t)count * ops->ctx_bytes);
+    void* ctx = w.ctx.get((size_t)count * ops->ctx_bytes);
     ops->make_ctx(d_seeds + 2 * n, 3 * n, d_seeds, 3 * n, d_seeds + n, 3 * n, count, ctx, st);
     const uint64_t tree_bytes = ((2ull << th) - 1) * n;
-    TreeJob* hj = h_jobs_.as<TreeJob>(count);
+    TreeJob* hj = w.h_jobs.as<TreeJob>(count);
     for (uint32_t k = 0; k < count; k++) hj[k] = TreeJob{k, p.d - 1, 0, (uint64_t)k * tree_bytes};
-    TreeJob* dj = s_jobs_.as<TreeJob>(count);
+    TreeJob* dj = w.jobs.as<TreeJob>(count);
     XB_CUDA(cudaMemcpyAsync(dj, hj, count * sizeof(TreeJob), cudaMemcpyHostToDevice, st));
-    uint8_t* nodes = s_nodes_.as<uint8_t>(count * tree_bytes);
-    build_trees(ops, dj, count, (int)th, nodes, ctx, st);
+    uint8_t* nodes = w.nodes.as<uint8_t>(count * tree_bytes);
+    build_trees(ops, dj, count, (int)th, nodes, ctx, st, w);
     k_keypair_finish<<<count, 64, 0, st>>>(d_seeds, nodes, tree_bytes, level_offset((int)th, (int)th) * n, n,
                                           p.index_bytes, (uint32_t)p.sk_bytes, count, d_pk, d_sk);
     // the host job list is reused by the next call only after this one's
@@ -278,18 +308,18 @@ void Engine::keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count,
 // One launch sequence of verify (prep, then per layer: bucket, chains, L-tree,
 // root) over the signatures v selects, on stream st.
 void Engine::verify_sequence(const FamilyOps* ops, const xmss_params& p, const VerifyArgs& v, const void* ctx,
-                             cudaStream_t st)
+                             cudaStream_t st, bool on)
 {
     const uint32_t len = ops->len;
-    mark(kPrep, true, st);
+    mark(kPrep, true, st, on);
     ops->verify_prep(v, ctx, st);
-    mark(kPrep, false, st);
+    mark(kPrep, false, st, on);
     for (uint32_t layer = 0; layer < p.d; layer++) {
-        mark(kChains, true, st);
+        mark(kChains, true, st, on);
         ops->verify_scatter(v, layer, st);
         ops->verify_chains(v, layer, ctx, st);
-        mark(kChains, false, st);
-        mark(kLtree, true, st);
+        mark(kChains, false, st, on);
+        mark(kLtree, true, st, on);
         int cnt = (int)len;
         uint32_t node_base = 0;
         uint8_t *src = v.wpk, *dst = v.wpk2;
@@ -301,21 +331,25 @@ void Engine::verify_sequence(const FamilyOps* ops, const xmss_params& p, const V
             std::swap(src, dst);
             std::swap(sstr, dstr);
         }
-        mark(kLtree, false, st);
-        mark(kRoot, true, st);
+        mark(kLtree, false, st, on);
+        mark(kRoot, true, st, on);
         ops->verify_root(v, layer, st);
-        mark(kRoot, false, st);
+        mark(kRoot, false, st, on);
     }
 }
 
 void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_sm,
                     const uint64_t* d_sm_off, const uint64_t* d_smlen, const uint8_t* d_pk, uint32_t npk,
-                    const uint32_t* d_pk_index, int* d_status, cudaStream_t st)
+                    const uint32_t* d_pk_index, int* d_status, cudaStream_t st, Workspace& w, bool allow_split)
 {
-    XB_CUDA(cudaMemsetAsync(work_, 0, 3 * sizeof(unsigned long long), st));
+    // the engine's own calls report their work through xmss_b200_last_verify_work;
+    // other workspaces (server slots) count into their own buffer and record no marks
+    const bool own = &w == &ws_;
+    unsigned long long* work = own ? work_ : w.work.as<unsigned long long>(4);
+    XB_CUDA(cudaMemsetAsync(work, 0, 3 * sizeof(unsigned long long), st));
     if (!count) return;
     const uint32_t n = p.n, len = ops->len, nh = len - 1 + p.tree_height;
-    void* ctx = s_ctx_.get((size_t)npk * ops->ctx_bytes);
+    void* ctx = w.ctx.get((size_t)npk * ops->ctx_bytes);
     ops->make_ctx(d_pk + n, 2 * n, nullptr, 0, nullptr, 0, npk, ctx, st);
     VerifyArgs v;
     v.sm = d_sm;
@@ -324,22 +358,22 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
     v.key = d_pk_index;
     v.key_root = d_pk;
     v.key_stride = 2 * n;
-    v.node = s_node_.as<uint8_t>((size_t)count * n);
-    v.lens = s_lens_.as<uint8_t>((size_t)count * len);
-    v.idx = s_idx_.as<uint64_t>(count);
+    v.node = w.node.as<uint8_t>((size_t)count * n);
+    v.lens = w.lens.as<uint8_t>((size_t)count * len);
+    v.idx = w.idx.as<uint64_t>(count);
     v.status = d_status;
-    v.wpk = s_wpk_.as<uint8_t>((size_t)count * len * n);
-    v.wpk2 = s_wpk2_.as<uint8_t>((size_t)count * ((len + 1) / 2) * n);
-    v.leaf = s_leaf_.as<uint8_t>((size_t)count * n);
-    v.refs = s_refs_.as<LeafRef>(count);
-    v.hpre = s_hpre_.get((size_t)count * p.d * nh * ops->hpre_bytes);
-    uint32_t* hist = s_hist_.as<uint32_t>(2 * 32 * p.d + 2);  // two groups + 2 group sizes
-    uint32_t* list = s_list_.as<uint32_t>((size_t)count * len + 2 * (size_t)count);
+    v.wpk = w.wpk.as<uint8_t>((size_t)count * len * n);
+    v.wpk2 = w.wpk2.as<uint8_t>((size_t)count * ((len + 1) / 2) * n);
+    v.leaf = w.leaf.as<uint8_t>((size_t)count * n);
+    v.refs = w.refs.as<LeafRef>(count);
+    v.hpre = w.hpre.get((size_t)count * p.d * nh * ops->hpre_bytes);
+    uint32_t* hist = w.hist.as<uint32_t>(2 * 32 * p.d + 2);  // two groups + 2 group sizes
+    uint32_t* list = w.list.as<uint32_t>((size_t)count * len + 2 * (size_t)count);
     v.hist = hist;
     v.list = list;
     v.sel = nullptr;
     v.sel_n = nullptr;
-    v.work = work_;
+    v.work = work;
     v.count = count;
     v.index_bytes = p.index_bytes;
     v.sig_bytes = p.sig_bytes;
@@ -350,8 +384,8 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
     // H_msg is short start their chains at once while the long messages are
     // still being hashed (H_msg is a serial chain of compressions).  The
     // profiling pass keeps one sequence so each kernel's time is its own.
-    if (count < kSplitMin || profiling) {
-        verify_sequence(ops, p, v, ctx, st);
+    if (!allow_split || count < kSplitMin || profiling) {
+        verify_sequence(ops, p, v, ctx, st, own);
         return;
     }
     uint32_t* n2 = hist + 2 * 32 * p.d;
@@ -364,11 +398,11 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
     b.sel = sel_long;
     b.sel_n = n2 + 1;
     b.hist = hist + 32 * p.d;
-    b.list = s_list2_.as<uint32_t>((size_t)count * len);  // each group has its own chain list
+    b.list = w.list2.as<uint32_t>((size_t)count * len);  // each group has its own chain list
     XB_CUDA(cudaEventRecord(fork_, st));
     XB_CUDA(cudaStreamWaitEvent(aux_, fork_, 0));
-    verify_sequence(ops, p, b, ctx, aux_);
-    verify_sequence(ops, p, a, ctx, st);
+    verify_sequence(ops, p, b, ctx, aux_, own);
+    verify_sequence(ops, p, a, ctx, st, own);
     XB_CUDA(cudaEventRecord(join_, aux_));
     XB_CUDA(cudaStreamWaitEvent(st, join_, 0));
 }
@@ -382,7 +416,7 @@ void Engine::last_verify_work(unsigned long long out[3])
 
 void Engine::sign(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* h_sk,
                   const uint64_t* h_idx, uint8_t* d_sm, const uint64_t* d_sm_off, const uint64_t* d_mlen,
-                  cudaStream_t st)
+                  cudaStream_t st, Workspace& w)
 {
     if (!count) return;
     const uint32_t n = p.n, th = p.tree_height, d = p.d, ib = p.index_bytes;
@@ -427,31 +461,33 @@ void Engine::sign(const FamilyOps* ops, const xmss_params& p, uint32_t count, co
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t o_jobs = al(sz_keys), o_toff = o_jobs + al(sz_jobs), o_idx = o_toff + al(sz_toff),
                  o_key = o_idx + al(sz_idx), total = o_key + al(sz_key);
-    uint8_t* hs = h_jobs_.as<uint8_t>(total);
+    uint8_t* hs = w.h_jobs.as<uint8_t>(total);
     memcpy(hs, keymat.data(), sz_keys);
     memcpy(hs + o_jobs, jobs.data(), sz_jobs);
     memcpy(hs + o_toff, tree_off.data(), sz_toff);
     memcpy(hs + o_idx, h_idx, sz_idx);
     memcpy(hs + o_key, req_key.data(), sz_key);
-    uint8_t* ds = s_keys_.as<uint8_t>(total);
+    uint8_t* ds = w.keys.as<uint8_t>(total);
     XB_CUDA(cudaMemcpyAsync(ds, hs, total, cudaMemcpyHostToDevice, st));
     const uint8_t* dkeys = ds;
-    void* ctx = s_ctx_.get((size_t)nkeys * ops->ctx_bytes);
+    void* ctx = w.ctx.get((size_t)nkeys * ops->ctx_bytes);
     // key material rows: SK_SEED | SK_PRF | root | PUB_SEED
     ops->make_ctx(dkeys + 3 * n, 4 * n, dkeys, 4 * n, dkeys + n, 4 * n, nkeys, ctx, st);
-    uint8_t* nodes = s_nodes_.as<uint8_t>(njobs * tree_bytes);
-    build_trees(ops, (const TreeJob*)(ds + o_jobs), njobs, (int)th, nodes, ctx, st);
+    uint8_t* nodes = w.nodes.as<uint8_t>(njobs * tree_bytes);
+    build_trees(ops, (const TreeJob*)(ds + o_jobs), njobs, (int)th, nodes, ctx, st, w);
     SignArgs g;
     g.sm = d_sm;
     g.sm_off = d_sm_off;
     g.mlen = d_mlen;
+    g.msg = nullptr;  // messages follow the signatures in d_sm
+    g.msg_off = nullptr;
     g.idx = (const uint64_t*)(ds + o_idx);
     g.key = (const uint32_t*)(ds + o_key);
     g.key_root = dkeys + 2 * n;
     g.key_stride = 4 * n;
     g.tree_off = (const uint64_t*)(ds + o_toff);
     g.nodes = nodes;
-    g.lens = s_lens_.as<uint8_t>((size_t)count * d * ops->len);
+    g.lens = w.lens.as<uint8_t>((size_t)count * d * ops->len);
     g.count = count;
     g.index_bytes = ib;
     g.sig_bytes = p.sig_bytes;

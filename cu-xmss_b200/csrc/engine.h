@@ -9,6 +9,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/params.h"
@@ -46,10 +47,26 @@ class DevBuf {
     {
         return (T*)get(count * sizeof(T));
     }
+    void swap(DevBuf& o)
+    {
+        std::swap(p_, o.p_);
+        std::swap(cap_, o.cap_);
+        std::swap(order_, o.order_);
+        std::swap(ordered_, o.ordered_);
+    }
+    // Growth becomes stream-ordered on st (cudaFreeAsync / cudaMallocAsync)
+    // instead of waiting for the whole device: for buffers only st uses.
+    void order_on(cudaStream_t st)
+    {
+        order_ = st;
+        ordered_ = true;
+    }
 
    private:
     void* p_ = nullptr;
     size_t cap_ = 0;
+    cudaStream_t order_ = nullptr;
+    bool ordered_ = false;
 };
 
 // Pinned host buffer that only grows.
@@ -66,9 +83,25 @@ class PinnedBuf {
         return (T*)get(count * sizeof(T));
     }
 
+    // Growth doubles and keeps the old block alive (the owner guarantees
+    // no copy uses it), so it never waits for the device.
+    void keep_old_blocks() { keep_old_ = true; }
+
    private:
     void* p_ = nullptr;
     size_t cap_ = 0;
+    bool keep_old_ = false;
+    std::vector<void*> retired_;
+};
+
+// Scratch of one in-flight launch sequence.  The engine owns one for its
+// own entry points; the server gives each of its batch slots one, so
+// batches on different streams never share intermediate buffers.
+struct Workspace {
+    DevBuf ctx, jobs, refs, wpk, wpk2, nodes, keys, node, lens, idx, leaf, hpre, hist, list, list2, aux;
+    DevBuf work;  // verify work counters of non-engine workspaces
+    PinnedBuf h_jobs;
+    void order_on(cudaStream_t st);  // every buffer grows stream-ordered on st
 };
 
 class Engine {
@@ -91,17 +124,34 @@ class Engine {
     // Builds every subtree of `jobs` (all of height h): node arrays at
     // d_nodes + job.node_off, levels 0..h.  d_jobs is the device copy of jobs.
     void build_trees(const FamilyOps* ops, const TreeJob* d_jobs, uint32_t njobs, int h, uint8_t* d_nodes,
-                     const void* d_ctx, cudaStream_t st);
+                     const void* d_ctx, cudaStream_t st, Workspace& w);
+    void build_trees(const FamilyOps* ops, const TreeJob* d_jobs, uint32_t njobs, int h, uint8_t* d_nodes,
+                     const void* d_ctx, cudaStream_t st)
+    {
+        build_trees(ops, d_jobs, njobs, h, d_nodes, d_ctx, st, ws_);
+    }
 
     // Verify of `count` signed messages against npk public keys (root||seed).
     void verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_sm,
                 const uint64_t* d_sm_off, const uint64_t* d_smlen, const uint8_t* d_pk, uint32_t npk,
-                const uint32_t* d_pk_index, int* d_status, cudaStream_t st);
+                const uint32_t* d_pk_index, int* d_status, cudaStream_t st)
+    {
+        verify(ops, p, count, d_sm, d_sm_off, d_smlen, d_pk, npk, d_pk_index, d_status, st, ws_, true);
+    }
+    // With allow_split false the batch runs as one sequence on st only.
+    void verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_sm,
+                const uint64_t* d_sm_off, const uint64_t* d_smlen, const uint8_t* d_pk, uint32_t npk,
+                const uint32_t* d_pk_index, int* d_status, cudaStream_t st, Workspace& w, bool allow_split);
 
     // Key generation from seeds (count x 3n) into pk (count x 2n) and sk
     // (count x sk_bytes), no OID prefix.
     void keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_seeds, uint8_t* d_pk,
-                 uint8_t* d_sk, cudaStream_t st);
+                 uint8_t* d_sk, cudaStream_t st)
+    {
+        keypair(ops, p, count, d_seeds, d_pk, d_sk, st, ws_);
+    }
+    void keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_seeds, uint8_t* d_pk,
+                 uint8_t* d_sk, cudaStream_t st, Workspace& w);
 
     // Signing given per-request key material.  h_sk: count x sk_bytes (no
     // OID), already reflecting the reference's exhaustion handling; h_idx:
@@ -109,7 +159,13 @@ class Engine {
     // message already at sm_off + sig_bytes.
     void sign(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* h_sk,
               const uint64_t* h_idx, uint8_t* d_sm, const uint64_t* d_sm_off, const uint64_t* d_mlen,
-              cudaStream_t st);
+              cudaStream_t st)
+    {
+        sign(ops, p, count, h_sk, h_idx, d_sm, d_sm_off, d_mlen, st, ws_);
+    }
+    void sign(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* h_sk,
+              const uint64_t* h_idx, uint8_t* d_sm, const uint64_t* d_sm_off, const uint64_t* d_mlen,
+              cudaStream_t st, Workspace& w);
 
     void core_hash(const FamilyOps* ops, uint32_t count, const uint8_t* d_in, const uint64_t* d_off,
                    const uint64_t* d_len, uint8_t* d_out, cudaStream_t st);
@@ -117,7 +173,7 @@ class Engine {
     // Verify launch sequence over the signatures v selects (all when
     // v.sel is null), on one stream.
     void verify_sequence(const FamilyOps* ops, const xmss_params& p, const VerifyArgs& v, const void* ctx,
-                         cudaStream_t st);
+                         cudaStream_t st, bool marks = true);
     // Batches of at least kSplitMin signatures are verified as two groups
     // split at kShortHmsgBlocks hash blocks of H_msg.
     static constexpr uint32_t kSplitMin = 1024;
@@ -129,7 +185,7 @@ class Engine {
     // Phase timing (xmss_b200_profile / xmss_b200_phase_ms).
     enum Phase { kPrep = 0, kChains = 1, kLtree = 2, kRoot = 3, kTree = 4, kPhases = 5 };
     bool profiling = false;
-    void mark(int phase, bool start, cudaStream_t st);  // no-op unless profiling
+    void mark(int phase, bool start, cudaStream_t st, bool on = true);  // no-op unless profiling and on
     void phase_ms(double out[kPhases]);
 
     // Scratch for host-buffer entry points (guarded by mu).
@@ -143,10 +199,8 @@ class Engine {
     cudaStream_t aux_ = nullptr;  // second stream of split verify batches
     cudaEvent_t fork_ = nullptr, join_ = nullptr;
     bool have_done_ = false;
-    // pipeline scratch
-    DevBuf s_ctx_, s_jobs_, s_refs_, s_wpk_, s_wpk2_, s_nodes_, s_keys_, s_node_, s_lens_, s_idx_, s_leaf_,
-        s_work_, s_tree_off_, s_key_idx_, s_mlen_, s_hpre_, s_hist_, s_list_, s_list2_;
-    PinnedBuf h_jobs_;
+    Workspace ws_;  // scratch of the engine's own entry points
+    DevBuf s_work_;
     unsigned long long* work_ = nullptr;
     struct Mark {
         int phase;

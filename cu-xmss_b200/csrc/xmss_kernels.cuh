@@ -575,9 +575,11 @@ __global__ void __launch_bounds__(64) k_verify_root(VerifyArgs v, uint32_t layer
 // Sign (xmss_core.c:183-273) given built subtrees.
 // ---------------------------------------------------------------------------
 struct SignArgs {
-    uint8_t* sm;              // concatenated output buffers; M already at sm + sig_bytes
+    uint8_t* sm;              // concatenated output buffers; M at sm + sig_bytes unless msg is set
     const uint64_t* sm_off;   // [count]
     const uint64_t* mlen;     // [count]
+    const uint8_t* msg;       // optional: message i at msg + msg_off[i] (signatures then stand alone)
+    const uint64_t* msg_off;  // [count]
     const uint64_t* idx;      // [count] one-time index of each signature
     const uint32_t* key;      // [count]
     const uint8_t* key_root;  // public root of key k at key_root + k * key_stride
@@ -608,7 +610,7 @@ __global__ void k_sign_prep(SignArgs g, const typename F::Ctx* __restrict__ ctx)
     F::prf_r(R, c, idx);
     F::store(sm + g.index_bytes, R);
     F::load(root, g.key_root + (uint64_t)g.key[s] * g.key_stride);
-    hmsg<F>(mh, R, root, idx, sm + g.sig_bytes, g.mlen[s]);
+    hmsg<F>(mh, R, root, idx, g.msg ? g.msg + g.msg_off[s] : sm + g.sig_bytes, g.mlen[s]);
     const uint64_t wsb = (uint64_t)F::LEN * F::N;
     for (uint32_t layer = 0; layer < g.d; layer++) {
         const uint8_t* tn = g.nodes + g.tree_off[(uint64_t)s * g.d + layer];

@@ -111,6 +111,49 @@ lib.xmss_b200_profile.argtypes = [C.c_int]
 lib.xmss_b200_phase_ms.argtypes = [C.POINTER(C.c_double)]
 lib.xmss_b200_rate_probe.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
 
+
+class ServerConfig(C.Structure):
+    """xmss_b200_server_config (include/xmss_b200.h)."""
+
+    _fields_ = [("max_batch", C.c_uint32), ("slots", C.c_uint32), ("window_us", C.c_uint32),
+                ("reserved0", C.c_uint32), ("tree_pool_bytes", C.c_uint64), ("mem_reserve_bytes", C.c_uint64)]
+
+
+class Completion(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("ret", C.c_int32), ("kind", C.c_uint32), ("index", C.c_uint64),
+                ("latency_us", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "batches", "sign_groups", "verify_groups",
+                                          "largest_batch", "deferred_for_memory", "trees_built", "tree_hits",
+                                          "trees_evicted")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# xmss_b200_trace_item as a numpy record (same layout as the C struct)
+TRACE_DTYPE = np.dtype([("t_us", "<f8"), ("kind", "<u4"), ("key_id", "<u4"), ("mt", "<i4"), ("reserved0", "<u4"),
+                        ("in_ptr", "<u8"), ("inlen", "<u8"), ("sm_ptr", "<u8"), ("smlen_ptr", "<u8"),
+                        ("pk_ptr", "<u8")])
+assert TRACE_DTYPE.itemsize == 64
+
+_srvp = C.c_void_p
+lib.xmss_b200_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(_srvp)]
+lib.xmss_b200_server_destroy.argtypes = [_srvp]
+lib.xmss_b200_server_destroy.restype = None
+lib.xmss_b200_server_add_key.argtypes = [_srvp, C.c_int, C.c_void_p, _u32p]
+lib.xmss_b200_server_export_sk.argtypes = [_srvp, C.c_uint32, C.c_void_p]
+lib.xmss_b200_server_submit_sign.argtypes = [_srvp, C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                                             C.c_uint64]
+lib.xmss_b200_server_submit_verify.argtypes = [_srvp, C.c_int, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64]
+lib.xmss_b200_server_submit_warm.argtypes = [_srvp, C.c_uint32, C.c_uint64]
+lib.xmss_b200_server_poll.argtypes = [_srvp, C.POINTER(Completion), C.c_uint32, C.c_uint32]
+lib.xmss_b200_server_stats_get.argtypes = [_srvp, C.POINTER(ServerStats)]
+lib.xmss_b200_server_replay.argtypes = [_srvp, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.POINTER(C.c_double)]
+
 PHASES = ("prep", "chains", "ltree", "root", "tree")
 
 
@@ -356,6 +399,23 @@ def sign_batch(mt: bool, sk: np.ndarray, msgs: Sequence[bytes]):
     return ret, sms
 
 
+def sign_batch_packed(mt: bool, sk: np.ndarray, mbuf: np.ndarray, moff: np.ndarray, mlen: np.ndarray,
+                      smbuf: np.ndarray, smoff: np.ndarray, smlen: np.ndarray, ret: np.ndarray) -> None:
+    """xmss_b200_sign_batch on arrays the caller packed (contiguous uint8 /
+    uint64 / int32, nothing copied): sk [count, 4+sk_bytes] is advanced in
+    place, sm i lands at smbuf[smoff[i]:smoff[i]+smlen[i]]."""
+    for a, t in ((sk, np.uint8), (mbuf, np.uint8), (moff, np.uint64), (mlen, np.uint64), (smbuf, np.uint8),
+                 (smoff, np.uint64), (smlen, np.uint64), (ret, np.int32)):
+        if a.dtype != t or not a.flags.c_contiguous:
+            raise TypeError("sign_batch_packed wants contiguous arrays of the documented dtypes")
+    r = _check(lib.xmss_b200_sign_batch(int(mt), sk.shape[0], _np_ptr(sk, C.c_uint8), _np_ptr(mbuf, C.c_uint8),
+                                        _np_ptr(moff, C.c_uint64), _np_ptr(mlen, C.c_uint64),
+                                        _np_ptr(smbuf, C.c_uint8), _np_ptr(smoff, C.c_uint64),
+                                        _np_ptr(smlen, C.c_uint64), _np_ptr(ret, C.c_int)), "sign_batch")
+    if r:
+        raise ValueError(f"sign_batch returned {r}: {last_error()}")
+
+
 def core_hash_batch(func: int, n: int, msgs: Sequence[bytes]) -> list[bytes]:
     buf, off, ln = pack(msgs)
     out = np.zeros((len(msgs), n), np.uint8)
@@ -410,3 +470,141 @@ def keypair_device(oid: int, mt: bool, count: int, d_seeds: int, d_pk: int, d_sk
     r = _check(lib.xmss_b200_keypair_device(oid, int(mt), count, d_seeds, d_pk, d_sk, stream), "keypair_device")
     if r:
         raise ValueError(f"keypair_device returned {r}: {last_error()}")
+
+
+# -- serving (xmss_b200_server_*) -------------------------------------------
+
+class Server:
+    """Request loop over device-resident keys (include/xmss_b200.h, serving).
+
+    submit_* return a tag; completions come back from poll() / wait() as
+    dicts {tag, ret, kind, index, latency_us} plus "sm" (bytes) for signs.
+    Buffers handed to the library are kept alive here until their request
+    completes."""
+
+    def __init__(self, max_batch: int = 0, slots: int = 0, window_us: int = 0, tree_pool_bytes: int = 0,
+                 mem_reserve_bytes: int = 0):
+        cfg = ServerConfig(max_batch, slots, window_us, 0, tree_pool_bytes, mem_reserve_bytes)
+        h = _srvp()
+        r = _check(lib.xmss_b200_server_create(C.byref(cfg), C.byref(h)), "server_create")
+        if r:
+            raise ValueError(f"server_create returned {r}")
+        self._h = h
+        self._next_tag = 1
+        self._pending: dict[int, tuple] = {}
+        self._sk_len: dict[int, int] = {}
+
+    def close(self) -> None:
+        if self._h:
+            lib.xmss_b200_server_destroy(self._h)
+            self._h = None
+            self._pending.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _tag(self) -> int:
+        t = self._next_tag
+        self._next_tag += 1
+        return t
+
+    def add_key(self, sk: bytes, mt: bool = False) -> int:
+        key_id = C.c_uint32()
+        b = _buf(sk)
+        r = _check(lib.xmss_b200_server_add_key(self._h, int(mt), b, C.byref(key_id)), "server_add_key")
+        if r:
+            raise ValueError(f"server_add_key returned {r}: {last_error()}")
+        self._sk_len[key_id.value] = len(sk)
+        return key_id.value
+
+    def export_sk(self, key_id: int) -> bytes:
+        out = _buf(self._sk_len[key_id])
+        r = lib.xmss_b200_server_export_sk(self._h, key_id, out)
+        if r:
+            raise ValueError(f"server_export_sk returned {r}")
+        return bytes(out)
+
+    def submit_sign(self, key_id: int, m: bytes, sig_bytes: int) -> int:
+        tag = self._tag()
+        mb = _buf(m)
+        smb = _buf(sig_bytes + len(m))
+        smlen = C.c_uint64()
+        r = lib.xmss_b200_server_submit_sign(self._h, key_id, mb, len(m), smb, C.byref(smlen), tag)
+        if r:
+            raise ValueError(f"server_submit_sign returned {r}")
+        self._pending[tag] = (mb, smb, smlen)
+        return tag
+
+    def submit_verify(self, sm: bytes, pk: bytes, mt: bool = False) -> int:
+        tag = self._tag()
+        smb = _buf(sm)
+        r = lib.xmss_b200_server_submit_verify(self._h, int(mt), smb, len(sm), _buf(pk), tag)
+        if r:
+            raise ValueError(f"server_submit_verify returned {r}")
+        self._pending[tag] = (smb,)
+        return tag
+
+    def submit_warm(self, key_id: int) -> int:
+        tag = self._tag()
+        r = lib.xmss_b200_server_submit_warm(self._h, key_id, tag)
+        if r:
+            raise ValueError(f"server_submit_warm returned {r}")
+        self._pending[tag] = ()
+        return tag
+
+    def poll(self, max_items: int = 4096, wait_us: int = 0) -> list[dict]:
+        arr = (Completion * max_items)()
+        n = lib.xmss_b200_server_poll(self._h, arr, max_items, wait_us)
+        out = []
+        for c in arr[:n]:
+            d = {"tag": c.tag, "ret": c.ret, "kind": c.kind, "index": c.index, "latency_us": c.latency_us}
+            keep = self._pending.pop(c.tag, None)
+            if c.kind == 0 and keep:
+                _, smb, smlen = keep
+                d["sm"] = bytes(smb)[:smlen.value] if c.ret == 0 else b""
+            out.append(d)
+        return out
+
+    def wait(self, tags, timeout_s: float = 120.0) -> dict[int, dict]:
+        """Polls until every tag in tags has completed; returns them by tag."""
+        import time
+        want = set(tags)
+        got: dict[int, dict] = {}
+        t_end = time.monotonic() + timeout_s
+        while want - got.keys():
+            if time.monotonic() > t_end:
+                raise TimeoutError(f"{len(want - got.keys())} requests still pending")
+            for d in self.poll(wait_us=20000):
+                got[d["tag"]] = d
+        return {t: got[t] for t in tags}
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        r = lib.xmss_b200_server_stats_get(self._h, C.byref(st))
+        if r:
+            raise GpuError(f"server failed: {last_error()}")
+        return st.as_dict()
+
+    def replay(self, trace: np.ndarray):
+        """xmss_b200_server_replay over a TRACE_DTYPE array (pointers inside must
+        stay valid).  Returns (ret int32, latency_us f64, index u64, elapsed_s)."""
+        trace = np.ascontiguousarray(trace, TRACE_DTYPE)
+        n = len(trace)
+        ret = np.full(n, -7, np.int32)
+        lat = np.zeros(n, np.float64)
+        idx = np.zeros(n, np.uint64)
+        el = C.c_double()
+        r = lib.xmss_b200_server_replay(self._h, trace.ctypes.data, n, ret.ctypes.data, lat.ctypes.data,
+                                        idx.ctypes.data, C.byref(el))
+        if r:
+            raise ValueError(f"server_replay returned {r}")
+        return ret, lat, idx, el.value

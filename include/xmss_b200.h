@@ -126,6 +126,122 @@ int xmss_b200_sign_open_device_noalloc(uint32_t oid, int mt, uint32_t count, con
                                        const uint8_t *d_pk, uint32_t npk, const uint32_t *d_pk_index,
                                        int *d_status, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Serving: a request loop over device-resident keys.  No reference
+ * counterpart as a whole; each request does what one xmss[mt]_sign
+ * (xmss.c:28-43, 78-93) or xmss[mt]_sign_open (xmss.c:45-60, 95-109) call
+ * does, with byte-identical results.
+ *
+ * Requests are submitted from any thread and complete asynchronously.  A
+ * dispatcher thread batches whatever is queued whenever one of `slots` batch
+ * slots is free (continuous batching: batches admitted while others run
+ * overlap on the device), groups each batch by operation and parameter set,
+ * and admits it only while free device memory (cudaMemGetInfo) stays above
+ * mem_reserve_bytes, shrinking the batch when it does not fit.
+ *
+ * Keys are resident on the device: seeds, PRF key, root, PUB_SEED, a u64
+ * one-time index counter advanced with atomicAdd (reservations run in
+ * submission order, so request i of a key gets the i-th index), and a cache
+ * of the subtrees signing needs (each built once, then authentication paths
+ * are copied out of it instead of recomputed as xmss_core.c:253-270 does).
+ * Indices run from the sk's index to 2^h - 2; the request that would take
+ * 2^h - 1 (signed with a wiped key by the reference, xmss_core.c:212-231)
+ * and all after it complete with -2.
+ *
+ * Completion codes: 0 ok (sign) / valid (verify); -1 invalid signature or
+ * bad request; -2 key exhausted; -3 resource or GPU failure.
+ * --------------------------------------------------------------------------- */
+typedef struct xmss_b200_server xmss_b200_server;
+
+typedef struct {
+    uint32_t max_batch;          /* requests per batch (default 4096) */
+    uint32_t slots;              /* batches in flight (default 4) */
+    uint32_t window_us;          /* a free slot waits up to this long for a batch to fill (default 0) */
+    uint32_t reserved0;
+    uint64_t tree_pool_bytes;    /* device memory of the subtree cache (default 1 GiB) */
+    uint64_t mem_reserve_bytes;  /* device memory admission leaves free (default 1 GiB) */
+} xmss_b200_server_config;
+
+typedef struct {
+    uint64_t tag;       /* as submitted */
+    int32_t ret;        /* completion code */
+    uint32_t kind;      /* 0 sign, 1 verify, 2 warm */
+    uint64_t index;     /* sign: the one-time index used */
+    double latency_us;  /* submission to completion */
+} xmss_b200_completion;
+
+typedef struct {
+    uint64_t submitted, completed;
+    uint64_t batches;          /* slot launches */
+    uint64_t sign_groups;      /* per-parameter-set sign launches */
+    uint64_t verify_groups;    /* per-parameter-set verify launches */
+    uint64_t largest_batch;
+    uint64_t deferred_for_memory;
+    uint64_t trees_built, tree_hits, trees_evicted;
+} xmss_b200_server_stats;
+
+/* cfg NULL or zero fields: defaults.  0 ok, -3 failure. */
+int xmss_b200_server_create(const xmss_b200_server_config *cfg, xmss_b200_server **out);
+
+/* Completes every submitted request (results are written to the callers'
+ * buffers, completions not yet polled are dropped), then frees the server. */
+void xmss_b200_server_destroy(xmss_b200_server *srv);
+
+/* Makes a secret key resident: sk is OID-prefixed as xmss[mt]_keypair writes
+ * it (xmss.c:18-25).  The server owns the key's state from here on; read it
+ * back with xmss_b200_server_export_sk.  0 ok, -1 unknown OID, -3 failure. */
+int xmss_b200_server_add_key(xmss_b200_server *srv, int mt, const uint8_t *sk, uint32_t *key_id);
+
+/* Writes the key's current sk (OID-prefixed, index = the next index the
+ * server would issue) to sk (4 + sk_bytes bytes).  Indices of requests still
+ * queued are not counted: export after they complete. */
+int xmss_b200_server_export_sk(xmss_b200_server *srv, uint32_t key_id, uint8_t *sk);
+
+/* Signs m (mlen bytes) with resident key key_id: writes sig || m to sm
+ * (capacity sig_bytes + mlen) and its length to *smlen.  m, sm and smlen
+ * must stay valid until the request completes. */
+int xmss_b200_server_submit_sign(xmss_b200_server *srv, uint32_t key_id, const uint8_t *m, uint64_t mlen,
+                                 uint8_t *sm, uint64_t *smlen, uint64_t tag);
+
+/* Verifies sm (smlen bytes) under pk (OID-prefixed, copied at submission);
+ * sm must stay valid until the request completes. */
+int xmss_b200_server_submit_verify(xmss_b200_server *srv, int mt, const uint8_t *sm, uint64_t smlen,
+                                   const uint8_t *pk, uint64_t tag);
+
+/* Builds (or keeps) the subtrees key_id's next signature needs, without
+ * taking an index: the cache rebuild after a key is added or restored.
+ * Completes as kind 2. */
+int xmss_b200_server_submit_warm(xmss_b200_server *srv, uint32_t key_id, uint64_t tag);
+
+/* Takes up to max completions, waiting up to wait_us for the first.
+ * Returns how many were written. */
+int xmss_b200_server_poll(xmss_b200_server *srv, xmss_b200_completion *out, uint32_t max, uint32_t wait_us);
+
+/* 0 ok, -3 when the dispatcher has failed (text in xmss_b200_last_error()). */
+int xmss_b200_server_stats_get(xmss_b200_server *srv, xmss_b200_server_stats *out);
+
+/* Load generator: submits items (sorted by t_us) at their times from a
+ * submitting thread while this thread polls, until all complete.  Latency is
+ * measured from each item's scheduled time, so a submitter that falls behind
+ * shows in the numbers.  ret[i], latency_us[i] and index[i] (sign: the index
+ * used) get item i's result; *elapsed_s the time from start to the last
+ * completion.  0 ok, -1 bad argument. */
+typedef struct {
+    double t_us;            /* scheduled submission time, from the start */
+    uint32_t kind;          /* 0 sign, 1 verify */
+    uint32_t key_id;        /* sign: resident key */
+    int32_t mt;             /* verify: 1 for XMSS^MT */
+    uint32_t reserved0;
+    const uint8_t *in;      /* sign: message; verify: signed message */
+    uint64_t inlen;
+    uint8_t *sm;            /* sign: output, capacity sig_bytes + inlen */
+    uint64_t *smlen;        /* sign: output length */
+    const uint8_t *pk;      /* verify: OID-prefixed public key */
+} xmss_b200_trace_item;
+
+int xmss_b200_server_replay(xmss_b200_server *srv, const xmss_b200_trace_item *items, uint32_t count, int *ret,
+                            double *latency_us, uint64_t *index, double *elapsed_s);
+
 /* Compression-rate probe (the roofline denominator): `blocks` x 128 threads
  * each run `iters` dependent SHA-256 compressions (kind 0) or Keccak-f[1600]
  * permutations (kind 1) in registers, on `stream`.  d_sink: blocks x 128
