@@ -862,8 +862,84 @@ __device__ __forceinline__ uint32_t stream_le(const HMsgPrefix<F>& pre, const ui
     return fetch4_le(m, mlen, 4 * (k - HMsgPrefix<F>::W));
 }
 
-// SHA-256 / SHA-512 / SHAKE streaming over the padded message.
-template <class F, int KIND>  // KIND 0 = SHA-256, 1 = SHA-512, 2 = SHAKE (rate from F)
+// SHA-256 / SHA-512 / SHAKE streaming over the padded stream prefix || M,
+// cut into blocks of BW 32-bit words (16 for SHA-256, 32 for SHA-512, the
+// rate for SHAKE).  H_msg is a serial chain of compressions per thread, so
+// its latency is the cost of one block times the blocks:
+//   * head blocks (those holding prefix words) are unrolled, so the prefix
+//     stays in registers;
+//   * body blocks lie inside M with a word to spare: BW + 1 aligned words
+//     are loaded one block ahead of the compression that consumes them and
+//     funnel-shifted into place (M need not be 4-byte aligned);
+//   * the tail blocks (end of M, padding, length) use bounded loads.
+// absorb(w, last) consumes one block of little-endian packed words (bytes
+// in stream order); pad(o, L) gives the padding bits of the word at stream
+// byte o of a stream of L bytes.
+template <int BW>
+__device__ __forceinline__ void body_load(uint32_t (&a)[BW + 1], const uint32_t* q, uint64_t j0)
+{
+#pragma unroll
+    for (int i = 0; i <= BW; i++) a[i] = __ldg(q + j0 + i);
+}
+
+template <class F, int BW, class Absorb, class Pad>
+__device__ __forceinline__ void hmsg_stream(const HMsgPrefix<F>& pre, const uint8_t* m, uint64_t mlen, uint64_t nb,
+                                            Absorb&& absorb, Pad&& pad)
+{
+    constexpr int W = HMsgPrefix<F>::W;
+    constexpr int PB = (W + BW - 1) / BW;  // blocks holding prefix words
+    const uint64_t L = 4ull * W + mlen;
+    // bounded word s of the padded stream (little-endian packed)
+    auto bounded = [&](uint64_t s) -> uint32_t {
+        const uint64_t o = 4 * s;
+        uint32_t le = (o < L) ? fetch4_le(m, mlen, o - 4ull * W) : 0;
+        return le | pad(o, L);
+    };
+#pragma unroll
+    for (int b = 0; b < PB; b++) {
+        if ((uint64_t)b < nb) {
+            uint32_t w[BW];
+#pragma unroll
+            for (int i = 0; i < BW; i++) {
+                const int s = b * BW + i;
+                if (s < W) {
+                    const uint32_t v = pre.w[s < W ? s : 0];
+                    w[i] = F::BE ? bswap32(v) : v;
+                } else {
+                    w[i] = bounded((uint64_t)s);
+                }
+            }
+            absorb(w, (uint64_t)b + 1 == nb);
+        }
+    }
+    // body: blocks b >= PB whose message words j0 .. j0 + BW (one spare)
+    // lie inside M, j0 = BW * b - W
+    const int64_t words = (int64_t)(mlen / 4);
+    const int64_t lim = words + W - BW - 1;
+    uint64_t bE = lim >= 0 ? (uint64_t)(lim / BW) + 1 : 0;
+    if (bE < (uint64_t)PB) bE = PB;
+    if (bE > nb) bE = nb;
+    const uintptr_t addr = (uintptr_t)m;
+    const uint32_t* q = (const uint32_t*)(addr & ~(uintptr_t)3);
+    const int sh = (int)(addr & 3) * 8;
+    uint32_t nxt[BW + 1];
+    if (bE > (uint64_t)PB) body_load<BW>(nxt, q, (uint64_t)BW * PB - W);
+    for (uint64_t b = PB; b < bE; b++) {
+        uint32_t w[BW];
+#pragma unroll
+        for (int i = 0; i < BW; i++) w[i] = __funnelshift_r(nxt[i], nxt[i + 1], sh);
+        if (b + 1 < bE) body_load<BW>(nxt, q, (uint64_t)BW * (b + 1) - W);
+        absorb(w, false);
+    }
+    for (uint64_t b = bE; b < nb; b++) {
+        uint32_t w[BW];
+#pragma unroll
+        for (int i = 0; i < BW; i++) w[i] = bounded((uint64_t)BW * b + i);
+        absorb(w, b + 1 == nb);
+    }
+}
+
+template <class F, int KIND>  // KIND 0 = SHA-256, 1 = SHA-512
 struct HMsgImpl;
 
 template <class F>
@@ -874,21 +950,18 @@ struct HMsgImpl<F, 0> {
         const uint64_t nb = (L + 9 + 63) / 64;
         uint32_t st[8];
         sha256_iv(st);
-        for (uint64_t b = 0; b < nb; b++) {
-            uint32_t w[16];
+        hmsg_stream<F, 16>(
+            pre, m, mlen, nb,
+            [&](uint32_t (&w)[16], bool last) {
 #pragma unroll
-            for (int j = 0; j < 16; j++) {
-                const uint64_t o = 64 * b + 4 * j;  // byte offset of this word
-                uint32_t le = (o < L) ? stream_le<F>(pre, m, mlen, o >> 2) : 0;
-                if (o <= L && L < o + 4) le |= 0x80u << (8 * (L - o));
-                w[j] = bswap32(le);
-            }
-            if (b == nb - 1) {
-                w[14] = (uint32_t)((L * 8) >> 32);
-                w[15] = (uint32_t)(L * 8);
-            }
-            sha256_compress(st, w);
-        }
+                for (int j = 0; j < 16; j++) w[j] = bswap32(w[j]);
+                if (last) {
+                    w[14] = (uint32_t)((L * 8) >> 32);
+                    w[15] = (uint32_t)(L * 8);
+                }
+                sha256_compress(st, w);
+            },
+            [](uint64_t o, uint64_t L_) -> uint32_t { return (o <= L_ && L_ < o + 4) ? 0x80u << (8 * (L_ - o)) : 0u; });
 #pragma unroll
         for (int i = 0; i < F::NW; i++) out[i] = st[i];
     }
@@ -902,26 +975,19 @@ struct HMsgImpl<F, 1> {
         const uint64_t nb = (L + 17 + 127) / 128;
         uint64_t st[8];
         sha512_iv(st);
-        for (uint64_t b = 0; b < nb; b++) {
-            uint64_t w[16];
+        hmsg_stream<F, 32>(
+            pre, m, mlen, nb,
+            [&](uint32_t (&w)[32], bool last) {
+                uint64_t w64[16];
 #pragma unroll
-            for (int j = 0; j < 16; j++) {
-                uint32_t hl[2];
-#pragma unroll
-                for (int q = 0; q < 2; q++) {
-                    const uint64_t o = 128 * b + 8 * j + 4 * q;
-                    uint32_t le = (o < L) ? stream_le<F>(pre, m, mlen, o >> 2) : 0;
-                    if (o <= L && L < o + 4) le |= 0x80u << (8 * (L - o));
-                    hl[q] = bswap32(le);
+                for (int j = 0; j < 16; j++) w64[j] = join64(bswap32(w[2 * j]), bswap32(w[2 * j + 1]));
+                if (last) {
+                    w64[14] = 0;
+                    w64[15] = L * 8;
                 }
-                w[j] = join64(hl[0], hl[1]);
-            }
-            if (b == nb - 1) {
-                w[14] = 0;
-                w[15] = L * 8;
-            }
-            sha512_compress(st, w);
-        }
+                sha512_compress(st, w64);
+            },
+            [](uint64_t o, uint64_t L_) -> uint32_t { return (o <= L_ && L_ < o + 4) ? 0x80u << (8 * (L_ - o)) : 0u; });
         uint32_t o16[16];
 #pragma unroll
         for (int i = 0; i < 8; i++) {
@@ -937,27 +1003,19 @@ template <class F, int RATEW>
 __device__ void hmsg_shake(uint32_t (&out)[F::NW], const HMsgPrefix<F>& pre, const uint8_t* m, uint64_t mlen)
 {
     const uint64_t L = 4ull * HMsgPrefix<F>::W + mlen;
-    const uint64_t RB = 4 * RATEW;
-    const uint64_t nb = L / RB + 1;
+    const uint64_t nb = L / (4 * RATEW) + 1;
     uint64_t A[25];
 #pragma unroll
     for (int i = 0; i < 25; i++) A[i] = 0;
-    for (uint64_t b = 0; b < nb; b++) {
+    hmsg_stream<F, RATEW>(
+        pre, m, mlen, nb,
+        [&](uint32_t (&w)[RATEW], bool last) {
+            if (last) w[RATEW - 1] ^= 0x80000000u;
 #pragma unroll
-        for (int i = 0; i < RATEW / 2; i++) {
-            uint32_t hl[2];
-#pragma unroll
-            for (int q = 0; q < 2; q++) {
-                const uint64_t o = RB * b + 8 * i + 4 * q;
-                uint32_t le = (o < L) ? stream_le<F>(pre, m, mlen, o >> 2) : 0;
-                if (o <= L && L < o + 4) le ^= 0x1Fu << (8 * (L - o));
-                hl[q] = le;
-            }
-            if (b == nb - 1 && 2 * i + 1 == RATEW - 1) hl[1] ^= 0x80000000u;
-            A[i] ^= ((uint64_t)hl[1] << 32) | hl[0];
-        }
-        keccak_f1600(A);
-    }
+            for (int i = 0; i < RATEW / 2; i++) A[i] ^= join64(w[2 * i + 1], w[2 * i]);
+            keccak_f1600(A);
+        },
+        [](uint64_t o, uint64_t L_) -> uint32_t { return (o <= L_ && L_ < o + 4) ? 0x1Fu << (8 * (L_ - o)) : 0u; });
 #pragma unroll
     for (int i = 0; i < F::NW; i++) out[i] = (i & 1) ? (uint32_t)(A[i / 2] >> 32) : (uint32_t)A[i / 2];
 }

@@ -157,10 +157,18 @@ struct Request {
     bool deferred = false;  // its subtrees did not fit the pool this time
 };
 
-struct Slot {
+// One stream of a slot with its own scratch: the plans of a batch (one per
+// operation and parameter set) run side by side on the slot's lanes.
+struct Lane {
     cudaStream_t st = nullptr;
-    cudaEvent_t done = nullptr, staged = nullptr, reserved = nullptr;
+    cudaEvent_t done = nullptr;
     xb::Workspace w;
+};
+
+struct Slot {
+    cudaStream_t st = nullptr;  // copies in and out; joins the lanes
+    cudaEvent_t done = nullptr, staged = nullptr, reserved = nullptr;
+    std::vector<std::unique_ptr<Lane>> lanes;
     xb::PinnedBuf stage;
     xb::DevBuf dev;
     bool busy = false;
@@ -169,6 +177,7 @@ struct Slot {
     bool any_sign = false;
     std::vector<std::unique_ptr<Request>> reqs;
     std::vector<TreeId> pinned, built;
+    Clock::time_point launched;
 };
 
 // One (operation, parameter set) group of a batch.
@@ -182,6 +191,7 @@ struct Plan {
     // sign
     std::vector<xb::TreeJob> jobs;
     std::vector<TreeId> job_ids;
+    std::vector<TreeId> used;  // every subtree its requests read
     std::vector<uint64_t> tree_off;  // [c][d]
     std::vector<uint32_t> grp, rank;
     // verify: distinct public keys
@@ -383,6 +393,7 @@ TreeEntry* xmss_b200_server::tree_for(uint32_t key_id, uint32_t layer, uint64_t 
         tree_hits++;
     }
     TreeEntry& e = it->second;
+    if (std::find(pl.used.begin(), pl.used.end(), id) == pl.used.end()) pl.used.push_back(id);
     e.last_use = ++use_clock;
     if (e.pinned_batch != batch_seq) {
         e.pinned_batch = batch_seq;
@@ -647,74 +658,87 @@ Launch xmss_b200_server::launch(Slot& s, std::vector<std::unique_ptr<Request>>& 
     XB_CUDA(cudaMemcpyAsync(d, h, in_end, cudaMemcpyHostToDevice, s.st));
     XB_CUDA(cudaMemsetAsync(mismatch_dev, 0, sizeof(int), s.st));
 
-    // ---- launch: new subtrees (each published by its event), the index
-    // reservation of all sign plans, then the plans ----
-    for (auto& kv : plans) {
-        Plan& pl = kv.second;
-        if (pl.kind != 0 || pl.jobs.empty()) continue;
-        engine->build_trees(pl.ops, (const TreeJob*)(d + pl.o_jobs), (uint32_t)pl.jobs.size(), (int)pl.p.tree_height,
-                            pool.as<uint8_t>(0), pl.table->ctx.as<uint8_t>(0), s.st, s.w);
-        for (const TreeId& id : pl.job_ids) XB_CUDA(cudaEventRecord(trees[id].ready, s.st));
-    }
-    for (const TreeId& id : s.pinned) {  // subtrees other slots are still building
-        const TreeEntry& e = trees[id];
-        if (!e.settled && std::find(s.built.begin(), s.built.end(), id) == s.built.end())
-            XB_CUDA(cudaStreamWaitEvent(s.st, e.ready, 0));
-    }
+    // ---- launch: the index reservation of all sign plans on the index
+    // stream, then each plan on its own lane (its new subtrees first, each
+    // published by its event), joined back into the slot's stream ----
+    XB_CUDA(cudaEventRecord(s.staged, s.st));
     if (G) {
-        XB_CUDA(cudaEventRecord(s.staged, s.st));
         XB_CUDA(cudaStreamWaitEvent(index_stream, s.staged, 0));
         k_serve_reserve<<<(G + 127) / 128, 128, 0, index_stream>>>((const uint64_t*)(d + o_gctr),
                                                                     (const uint32_t*)(d + o_gn), G,
                                                                     (unsigned long long*)(d + o_base));
         XB_CUDA(cudaEventRecord(s.reserved, index_stream));
-        XB_CUDA(cudaStreamWaitEvent(s.st, s.reserved, 0));
     }
     uint64_t groups_sign = 0, groups_verify = 0;
+    size_t nl = 0;
     for (auto& kv : plans) {
         Plan& pl = kv.second;
         const uint32_t c = (uint32_t)pl.reqs.size();
-        if (!c) continue;
+        if (!c && pl.jobs.empty()) continue;
+        if (nl == s.lanes.size()) {
+            auto ln = std::make_unique<Lane>();
+            XB_CUDA(cudaStreamCreateWithFlags(&ln->st, cudaStreamNonBlocking));
+            XB_CUDA(cudaEventCreateWithFlags(&ln->done, cudaEventDisableTiming));
+            ln->w.order_on(ln->st);
+            s.lanes.push_back(std::move(ln));
+        }
+        Lane& L = *s.lanes[nl++];
+        XB_CUDA(cudaStreamWaitEvent(L.st, s.staged, 0));
         const xmss_params& p = pl.p;
         if (pl.kind == 1) {
             engine->verify(pl.ops, p, c, d + pl.o_in, (const uint64_t*)(d + pl.o_off), (const uint64_t*)(d + pl.o_len),
                            d + pl.o_pk, (uint32_t)(pl.pks.size() / (2 * p.n)), (const uint32_t*)(d + pl.o_key),
-                           (int*)(d + pl.o_out), s.st, s.w, false);
+                           (int*)(d + pl.o_out), L.st, L.w, false);
             groups_verify++;
-            continue;
+        } else {
+            if (!pl.jobs.empty()) {
+                engine->build_trees(pl.ops, (const TreeJob*)(d + pl.o_jobs), (uint32_t)pl.jobs.size(),
+                                    (int)p.tree_height, pool.as<uint8_t>(0), pl.table->ctx.as<uint8_t>(0), L.st, L.w);
+                for (const TreeId& id : pl.job_ids) XB_CUDA(cudaEventRecord(trees[id].ready, L.st));
+            }
+            for (const TreeId& id : pl.used) {  // subtrees other slots are still building
+                const TreeEntry& e = trees[id];
+                if (!e.settled && std::find(pl.job_ids.begin(), pl.job_ids.end(), id) == pl.job_ids.end())
+                    XB_CUDA(cudaStreamWaitEvent(L.st, e.ready, 0));
+            }
+            if (c) {
+                XB_CUDA(cudaStreamWaitEvent(L.st, s.reserved, 0));
+                uint64_t* d_idx = (uint64_t*)(d + pl.o_idx);
+                k_serve_index<<<(c + 127) / 128, 128, 0, L.st>>>(
+                    (const unsigned long long*)(d + o_base), (const uint32_t*)(d + pl.o_grp),
+                    (const uint32_t*)(d + pl.o_rank), (const uint64_t*)(d + pl.o_plan), c, d_idx, mismatch_dev);
+                SignArgs g{};
+                g.sm = d + pl.o_out;
+                g.sm_off = (const uint64_t*)(d + pl.o_soff);
+                g.mlen = (const uint64_t*)(d + pl.o_len);
+                g.msg = d + pl.o_in;
+                g.msg_off = (const uint64_t*)(d + pl.o_off);
+                g.idx = d_idx;
+                g.key = (const uint32_t*)(d + pl.o_key);
+                g.key_root = pl.table->mat.as<uint8_t>(0) + 2 * p.n;
+                g.key_stride = 4 * p.n;
+                g.tree_off = (const uint64_t*)(d + pl.o_toff);
+                g.nodes = pool.as<uint8_t>(0);
+                g.lens = L.w.lens.as<uint8_t>((size_t)c * p.d * pl.ops->len);
+                g.count = c;
+                g.index_bytes = p.index_bytes;
+                g.sig_bytes = p.sig_bytes;
+                g.tree_height = p.tree_height;
+                g.d = p.d;
+                pl.ops->sign_prep(g, pl.table->ctx.as<uint8_t>(0), L.st);
+                pl.ops->sign_chains(g, pl.table->ctx.as<uint8_t>(0), L.st);
+                groups_sign++;
+            }
         }
-        uint64_t* d_idx = (uint64_t*)(d + pl.o_idx);
-        k_serve_index<<<(c + 127) / 128, 128, 0, s.st>>>((const unsigned long long*)(d + o_base),
-                                                          (const uint32_t*)(d + pl.o_grp),
-                                                          (const uint32_t*)(d + pl.o_rank),
-                                                          (const uint64_t*)(d + pl.o_plan), c, d_idx, mismatch_dev);
-        SignArgs g{};
-        g.sm = d + pl.o_out;
-        g.sm_off = (const uint64_t*)(d + pl.o_soff);
-        g.mlen = (const uint64_t*)(d + pl.o_len);
-        g.msg = d + pl.o_in;
-        g.msg_off = (const uint64_t*)(d + pl.o_off);
-        g.idx = d_idx;
-        g.key = (const uint32_t*)(d + pl.o_key);
-        g.key_root = pl.table->mat.as<uint8_t>(0) + 2 * p.n;
-        g.key_stride = 4 * p.n;
-        g.tree_off = (const uint64_t*)(d + pl.o_toff);
-        g.nodes = pool.as<uint8_t>(0);
-        g.lens = s.w.lens.as<uint8_t>((size_t)c * p.d * pl.ops->len);
-        g.count = c;
-        g.index_bytes = p.index_bytes;
-        g.sig_bytes = p.sig_bytes;
-        g.tree_height = p.tree_height;
-        g.d = p.d;
-        pl.ops->sign_prep(g, pl.table->ctx.as<uint8_t>(0), s.st);
-        pl.ops->sign_chains(g, pl.table->ctx.as<uint8_t>(0), s.st);
-        groups_sign++;
+        XB_CUDA(cudaEventRecord(L.done, L.st));
+        XB_CUDA(cudaStreamWaitEvent(s.st, L.done, 0));
     }
     XB_CUDA(cudaMemcpyAsync(h + out_begin, d + out_begin, total - out_begin, cudaMemcpyDeviceToHost, s.st));
     XB_CUDA(cudaGetLastError());
     XB_CUDA(cudaEventRecord(s.done, s.st));
     s.admitted = std::max(s.admitted, est);
     s.any_sign = G != 0;
+    s.launched = Clock::now();
     s.reqs = std::move(reqs);
     s.busy = true;
     std::lock_guard<std::mutex> lk(mu);
@@ -728,6 +752,7 @@ Launch xmss_b200_server::launch(Slot& s, std::vector<std::unique_ptr<Request>>& 
 // Copies a finished slot's results out and completes its requests.
 void xmss_b200_server::finish(Slot& s)
 {
+    const Clock::time_point t0 = Clock::now();
     const uint8_t* h = s.stage.as<uint8_t>(1);
     const bool mismatch = s.any_sign && *s.mismatch != 0;
     copies->run(s.reqs.size(), [&](size_t i) {
@@ -750,6 +775,8 @@ void xmss_b200_server::finish(Slot& s)
     release(s);
     s.busy = false;
     std::lock_guard<std::mutex> lk(mu);
+    stats.batch_us += std::chrono::duration<double, std::micro>(t0 - s.launched).count();
+    stats.finish_us += std::chrono::duration<double, std::micro>(Clock::now() - t0).count();
     if (mismatch) fatal = "xmss_b200_server: device index counter differs from the plan";
     for (auto& rp : s.reqs) complete_locked(*rp);
     s.reqs.clear();
@@ -795,7 +822,12 @@ void xmss_b200_server::run()
         std::vector<std::unique_ptr<Request>> wait_pool;
         try {
             std::lock_guard<std::mutex> lk(launch_mu);
+            const Clock::time_point t0 = Clock::now();
             res = launch(*free_slot, take, wait_pool);
+            {
+                std::lock_guard<std::mutex> g(mu);
+                stats.launch_us += std::chrono::duration<double, std::micro>(Clock::now() - t0).count();
+            }
             if (res == Launch::kNothing) {  // refused while planning, or warm and cached
                 release(*free_slot);
                 std::lock_guard<std::mutex> g(mu);
@@ -934,7 +966,6 @@ extern "C" int xmss_b200_server_create(const xmss_b200_server_config* cfg, xmss_
             XB_CUDA(cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming));
             XB_CUDA(cudaEventCreateWithFlags(&s->staged, cudaEventDisableTiming));
             XB_CUDA(cudaEventCreateWithFlags(&s->reserved, cudaEventDisableTiming));
-            s->w.order_on(s->st);
             s->dev.order_on(s->st);
             s->stage.keep_old_blocks();
             s->stage.get(64ull << 20);
@@ -964,6 +995,11 @@ extern "C" void xmss_b200_server_destroy(xmss_b200_server* srv)
     if (srv->thread.joinable()) srv->thread.join();
     cudaSetDevice(srv->device);
     for (auto& s : srv->slots) {
+        for (auto& ln : s->lanes) {
+            cudaStreamSynchronize(ln->st);
+            cudaEventDestroy(ln->done);
+            cudaStreamDestroy(ln->st);
+        }
         cudaEventDestroy(s->done);
         cudaEventDestroy(s->staged);
         cudaEventDestroy(s->reserved);

@@ -127,7 +127,8 @@ class Completion(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "batches", "sign_groups", "verify_groups",
                                           "largest_batch", "deferred_for_memory", "trees_built", "tree_hits",
-                                          "trees_evicted")]
+                                          "trees_evicted")] + [
+        ("launch_us", C.c_double), ("finish_us", C.c_double), ("batch_us", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -178,6 +178,9 @@ typedef struct {
     uint64_t largest_batch;
     uint64_t deferred_for_memory;
     uint64_t trees_built, tree_hits, trees_evicted;
+    double launch_us;  /* dispatcher time planning, staging and launching */
+    double finish_us;  /* dispatcher time copying results out */
+    double batch_us;   /* summed launch-to-completion time of the batches */
 } xmss_b200_server_stats;
 
 /* cfg NULL or zero fields: defaults.  0 ok, -3 failure. */

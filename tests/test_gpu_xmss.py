@@ -228,3 +228,46 @@ def test_large_batch_two_group_path(xb, oracle):
     assert (st == expect).all()
     for i in rng.choice(count, 40, replace=False):
         assert oracle.sign_open(po, sms[i], bytes(pks[keyix[i], 4:]))[0] == st[i]
+
+
+def test_hmsg_block_edges_every_family(xb, oracle, golden):
+    """H_msg streams prefix || M block by block (prefix blocks unrolled, body
+    blocks prefetched and funnel-shifted, bounded tail).  For every hash
+    family, message lengths around each block, rate and padding edge up to
+    70 KB, signed at unaligned message offsets (XMSS^MT 20/4: 3 index bytes),
+    must equal the oracle's signatures, and verify - with the message
+    starting at any byte offset - must accept them and reject a bit flip at
+    the start, middle or end of the message."""
+    lengths = [0, 1, 2, 3, 5, 31, 63, 64, 65, 100, 127, 128, 129, 135, 136, 137, 167, 168, 169, 200, 255, 256,
+               257, 300, 1000, 1023, 4099, 70001]
+    rng = np.random.default_rng(77)
+    for k in golden("mt_small.json"):
+        p, po = xb.parse_oid(k["oid"], True), oracle.params(k["oid"], True)
+        pk, sk = bytes.fromhex(k["pk"]), bytes.fromhex(k["sk"])
+        oidb = k["oid"].to_bytes(4, "big")
+        msgs = [rng.bytes(L) for L in lengths]
+        idx = rng.integers(0, (1 << 20) - 1, len(msgs))
+        rows = np.zeros((len(msgs), 4 + len(sk)), np.uint8)
+        for i in range(len(msgs)):
+            rows[i] = np.frombuffer(oidb + int(idx[i]).to_bytes(p.index_bytes, "big") + sk[p.index_bytes:], np.uint8)
+        ret, sms = xb.sign_batch(True, rows.copy(), msgs)
+        for i, m in enumerate(msgs):
+            want = oracle.sign(po, bytes(rows[i, 4:]), m)[2]
+            assert ret[i] == 0 and sms[i] == want, (k["oid"], len(m))
+        variants, expect = [], []
+        for sm, m in zip(sms, msgs):
+            variants.append(sm)
+            expect.append(0)
+            for pos in (0, len(m) // 2, len(m) - 1) if m else ():
+                b = bytearray(sm)
+                b[p.sig_bytes + pos] ^= 1 << int(rng.integers(0, 8))
+                variants.append(bytes(b))
+                expect.append(-1)
+        # byte offsets 0, 1, 2, 3, ... mod 4 for the signed messages
+        pad = [rng.bytes(int(rng.integers(0, 4))) for _ in variants]
+        buf, off, ln = xb.pack([q + v for q, v in zip(pad, variants)])
+        off = off + np.array([len(q) for q in pad], np.uint64)
+        ln = ln - np.array([len(q) for q in pad], np.uint64)
+        pkarr = np.frombuffer(oidb + pk, np.uint8)[None, :]
+        st = xb.sign_open_batch(True, buf, off, ln, pkarr, np.zeros(len(variants), np.uint32))
+        assert list(st) == expect, k["oid"]
