@@ -763,12 +763,21 @@ def run_serve(args):
             "pk": pkt, "pk_stride": pk_stride}
     log("serve: pool ready", srv.stats())
 
+    # warm-up (untimed): a burst that grows every slot's and lane's buffers
+    # to their working size before the sweep
+    tr, keep = _serve_trace(xb, rng, args.serve_n // 2, 0.0, keys, kids, pool, rand)
+    ret, _, _, _ = srv.replay(tr)
+    assert (ret == 0).all()
+    log("serve: warm", srv.stats())
+
     rates = [float(r) for r in args.serve_rates.split(",")]
     sweep = []
     for rate in rates + [0.0]:
         n = args.serve_n if rate == 0 else int(min(args.serve_n, max(2000, rate * args.serve_seconds)))
         tr, keep = _serve_trace(xb, rng, n, rate, keys, kids, pool, rand)
+        seq0 = max([b["seq"] for b in srv.batch_trace(1)], default=0)
         ret, lat, idx, el = srv.replay(tr)
+        bt = [b for b in srv.batch_trace() if b["seq"] > seq0]
         out, smlen, sign, k, out_off, mlen, moff = keep
         ok = bool((ret == 0).all())
         # spot-check: signatures byte-for-byte verified by the batch API
@@ -790,6 +799,20 @@ def run_serve(args):
                "p99_sign_ms": float(np.percentile(lat_ms[sign], 99)),
                "p99_verify_ms": float(np.percentile(lat_ms[~sign], 99)),
                "mean_mlen": float(np.mean(mlen))}
+        if bt:
+            slow = {}
+            for b in bt:
+                key = f"{'sign' if b['slow_kind'] == 0 else 'verify'}:{b['slow_oid']:#x}"
+                slow[key] = slow.get(key, 0) + 1
+            row["batches"] = {"count": len(bt), "mean_requests": float(np.mean([b["requests"] for b in bt])),
+                              **{f"p50_{f}": float(np.percentile([b[f] for b in bt], 50))
+                                 for f in ("queue_us", "launch_us", "gpu_us", "lane_us", "done_us", "start_skew_us",
+                                           "join_us")},
+                              **{f"p99_{f}": float(np.percentile([b[f] for b in bt], 99))
+                                 for f in ("queue_us", "launch_us", "gpu_us", "lane_us", "done_us")},
+                              **{f"max_{f}": float(np.max([b[f] for b in bt]))
+                                 for f in ("queue_us", "launch_us", "gpu_us", "done_us")},
+                              "slowest_lane": slow}
         sweep.append(row)
         log(row)
     stats = srv.stats()

@@ -127,6 +127,11 @@ Engine& Engine::get()
     static Engine* e = nullptr;
     std::lock_guard<std::mutex> g(m);
     if (!e) {
+        // The server runs up to ~30 streams at once; with the runtime's
+        // default of 8 hardware work queues unrelated streams share a queue
+        // and wait behind each other's kernels.  Effective only when this is
+        // the process's first CUDA call; a caller's own setting wins.
+        setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
         int dev = 0;
         const char* env = getenv("XMSS_B200_DEVICE");
         if (env) {

@@ -161,8 +161,9 @@ struct Request {
 // operation and parameter set) run side by side on the slot's lanes.
 struct Lane {
     cudaStream_t st = nullptr;
-    cudaEvent_t done = nullptr;
+    cudaEvent_t start = nullptr, done = nullptr;  // timing events
     xb::Workspace w;
+    uint32_t kind = 0, oid = 0;  // plan of the current batch
 };
 
 struct Slot {
@@ -178,11 +179,14 @@ struct Slot {
     std::vector<std::unique_ptr<Request>> reqs;
     std::vector<TreeId> pinned, built;
     Clock::time_point launched;
+    size_t lanes_used = 0;
+    xmss_b200_batch_trace trace{};  // filled at launch, completed at finish
 };
 
 // One (operation, parameter set) group of a batch.
 struct Plan {
     uint32_t kind = 0;  // 0 sign (warm requests ride along), 1 verify
+    uint32_t oid = 0;
     xmss_params p{};
     const xb::FamilyOps* ops = nullptr;
     KeyTable* table = nullptr;
@@ -203,6 +207,23 @@ struct Plan {
 };
 
 enum class Launch { kLaunched, kNothing, kDeferred };
+
+// Lanes per slot: slots x (lanes + 1) + 1 streams stay within the 32
+// hardware work queues of the device.
+constexpr size_t kMaxLanes = 6;
+
+// Estimated critical path of a plan in microseconds on an idle GPU: the
+// fixed pipeline depth of its family (chains, L-tree and root levels per
+// layer) plus its longest H_msg, a serial chain of compressions
+// (lone-thread latency per block: SHA-256 ~1.8, SHA-512 ~6.8, Keccak ~6.2).
+double plan_cost_us(uint32_t kind, const xmss_params& p, uint64_t max_inlen)
+{
+    const bool sha2 = p.func == XMSS_SHA2;
+    const double per_block = sha2 ? (p.n == 64 ? 6.8 : 1.8) : 6.2;
+    const double block = sha2 ? (p.n == 64 ? 128.0 : 64.0) : (p.n == 32 && p.func == XMSS_SHAKE128 ? 168.0 : 136.0);
+    const double depth = (sha2 ? (p.n == 64 ? 900.0 : 220.0) : 800.0) * (kind == 1 ? 1.3 : 1.0) * p.d;
+    return depth + per_block * ((double)max_inlen / block + 2);
+}
 
 // Host threads that share the byte copies of a batch (requests into the
 // pinned staging block, results out of it): one thread copies ~10 GB/s,
@@ -306,6 +327,7 @@ struct xmss_b200_server {
     std::vector<std::pair<uint64_t, uint64_t>> holes;  // free pool regions (off, cap)
     uint64_t use_clock = 0, batch_seq = 0;
     uint64_t trees_built = 0, tree_hits = 0, trees_evicted = 0;
+    std::deque<xmss_b200_batch_trace> traces;  // guarded by mu
     std::vector<std::unique_ptr<Slot>> slots;
     std::unique_ptr<CopyPool> copies;
     std::thread thread;
@@ -460,6 +482,7 @@ Launch xmss_b200_server::launch(Slot& s, std::vector<std::unique_ptr<Request>>& 
         Plan& pl = plans[{r.kind == 1 ? 1u : 0u, r.mt, r.oid}];
         if (!pl.ops) {
             pl.kind = r.kind == 1 ? 1 : 0;
+            pl.oid = r.oid;
             pl.p = r.p;
             pl.ops = family_ops(r.p.func, r.p.n);
             if (pl.kind == 0) pl.table = keys[r.key_id]->table;
@@ -670,64 +693,89 @@ Launch xmss_b200_server::launch(Slot& s, std::vector<std::unique_ptr<Request>>& 
         XB_CUDA(cudaEventRecord(s.reserved, index_stream));
     }
     uint64_t groups_sign = 0, groups_verify = 0;
-    size_t nl = 0;
+    // plans onto lanes, longest first onto the least loaded lane (a lane
+    // runs its plans one after the other)
+    std::vector<std::pair<double, Plan*>> order;
     for (auto& kv : plans) {
         Plan& pl = kv.second;
-        const uint32_t c = (uint32_t)pl.reqs.size();
-        if (!c && pl.jobs.empty()) continue;
-        if (nl == s.lanes.size()) {
-            auto ln = std::make_unique<Lane>();
-            XB_CUDA(cudaStreamCreateWithFlags(&ln->st, cudaStreamNonBlocking));
-            XB_CUDA(cudaEventCreateWithFlags(&ln->done, cudaEventDisableTiming));
-            ln->w.order_on(ln->st);
-            s.lanes.push_back(std::move(ln));
-        }
-        Lane& L = *s.lanes[nl++];
+        if (pl.reqs.empty() && pl.jobs.empty()) continue;
+        uint64_t longest = 0;
+        for (Request* r : pl.reqs) longest = std::max(longest, r->inlen);
+        double cost = plan_cost_us(pl.kind, pl.p, longest);
+        if (!pl.jobs.empty()) cost += 1e6;  // subtree builds: alone on a lane, first
+        order.emplace_back(cost, &pl);
+    }
+    std::sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    const size_t nl = std::min(order.size(), kMaxLanes);
+    while (s.lanes.size() < nl) {
+        auto ln = std::make_unique<Lane>();
+        XB_CUDA(cudaStreamCreateWithFlags(&ln->st, cudaStreamNonBlocking));
+        XB_CUDA(cudaEventCreate(&ln->start));
+        XB_CUDA(cudaEventCreate(&ln->done));
+        ln->w.order_on(ln->st);
+        s.lanes.push_back(std::move(ln));
+    }
+    std::vector<double> load(nl, 0.0);
+    std::vector<std::vector<Plan*>> lane_plans(nl);
+    for (auto& [cost, pl] : order) {
+        const size_t i = std::min_element(load.begin(), load.end()) - load.begin();
+        load[i] += cost;
+        lane_plans[i].push_back(pl);
+    }
+    for (size_t li = 0; li < nl; li++) {
+        Lane& L = *s.lanes[li];
         XB_CUDA(cudaStreamWaitEvent(L.st, s.staged, 0));
-        const xmss_params& p = pl.p;
-        if (pl.kind == 1) {
-            engine->verify(pl.ops, p, c, d + pl.o_in, (const uint64_t*)(d + pl.o_off), (const uint64_t*)(d + pl.o_len),
-                           d + pl.o_pk, (uint32_t)(pl.pks.size() / (2 * p.n)), (const uint32_t*)(d + pl.o_key),
-                           (int*)(d + pl.o_out), L.st, L.w, false);
-            groups_verify++;
-        } else {
-            if (!pl.jobs.empty()) {
-                engine->build_trees(pl.ops, (const TreeJob*)(d + pl.o_jobs), (uint32_t)pl.jobs.size(),
-                                    (int)p.tree_height, pool.as<uint8_t>(0), pl.table->ctx.as<uint8_t>(0), L.st, L.w);
-                for (const TreeId& id : pl.job_ids) XB_CUDA(cudaEventRecord(trees[id].ready, L.st));
-            }
-            for (const TreeId& id : pl.used) {  // subtrees other slots are still building
-                const TreeEntry& e = trees[id];
-                if (!e.settled && std::find(pl.job_ids.begin(), pl.job_ids.end(), id) == pl.job_ids.end())
-                    XB_CUDA(cudaStreamWaitEvent(L.st, e.ready, 0));
-            }
-            if (c) {
-                XB_CUDA(cudaStreamWaitEvent(L.st, s.reserved, 0));
-                uint64_t* d_idx = (uint64_t*)(d + pl.o_idx);
-                k_serve_index<<<(c + 127) / 128, 128, 0, L.st>>>(
-                    (const unsigned long long*)(d + o_base), (const uint32_t*)(d + pl.o_grp),
-                    (const uint32_t*)(d + pl.o_rank), (const uint64_t*)(d + pl.o_plan), c, d_idx, mismatch_dev);
-                SignArgs g{};
-                g.sm = d + pl.o_out;
-                g.sm_off = (const uint64_t*)(d + pl.o_soff);
-                g.mlen = (const uint64_t*)(d + pl.o_len);
-                g.msg = d + pl.o_in;
-                g.msg_off = (const uint64_t*)(d + pl.o_off);
-                g.idx = d_idx;
-                g.key = (const uint32_t*)(d + pl.o_key);
-                g.key_root = pl.table->mat.as<uint8_t>(0) + 2 * p.n;
-                g.key_stride = 4 * p.n;
-                g.tree_off = (const uint64_t*)(d + pl.o_toff);
-                g.nodes = pool.as<uint8_t>(0);
-                g.lens = L.w.lens.as<uint8_t>((size_t)c * p.d * pl.ops->len);
-                g.count = c;
-                g.index_bytes = p.index_bytes;
-                g.sig_bytes = p.sig_bytes;
-                g.tree_height = p.tree_height;
-                g.d = p.d;
-                pl.ops->sign_prep(g, pl.table->ctx.as<uint8_t>(0), L.st);
-                pl.ops->sign_chains(g, pl.table->ctx.as<uint8_t>(0), L.st);
-                groups_sign++;
+        XB_CUDA(cudaEventRecord(L.start, L.st));
+        L.kind = lane_plans[li].front()->kind;
+        L.oid = lane_plans[li].front()->oid;
+        for (Plan* plp : lane_plans[li]) {
+            Plan& pl = *plp;
+            const uint32_t c = (uint32_t)pl.reqs.size();
+            const xmss_params& p = pl.p;
+            if (pl.kind == 1) {
+                engine->verify(pl.ops, p, c, d + pl.o_in, (const uint64_t*)(d + pl.o_off), (const uint64_t*)(d + pl.o_len),
+                               d + pl.o_pk, (uint32_t)(pl.pks.size() / (2 * p.n)), (const uint32_t*)(d + pl.o_key),
+                               (int*)(d + pl.o_out), L.st, L.w, false);
+                groups_verify++;
+            } else {
+                if (!pl.jobs.empty()) {
+                    engine->build_trees(pl.ops, (const TreeJob*)(d + pl.o_jobs), (uint32_t)pl.jobs.size(),
+                                        (int)p.tree_height, pool.as<uint8_t>(0), pl.table->ctx.as<uint8_t>(0), L.st, L.w);
+                    for (const TreeId& id : pl.job_ids) XB_CUDA(cudaEventRecord(trees[id].ready, L.st));
+                }
+                for (const TreeId& id : pl.used) {  // subtrees other slots are still building
+                    const TreeEntry& e = trees[id];
+                    if (!e.settled && std::find(pl.job_ids.begin(), pl.job_ids.end(), id) == pl.job_ids.end())
+                        XB_CUDA(cudaStreamWaitEvent(L.st, e.ready, 0));
+                }
+                if (c) {
+                    XB_CUDA(cudaStreamWaitEvent(L.st, s.reserved, 0));
+                    uint64_t* d_idx = (uint64_t*)(d + pl.o_idx);
+                    k_serve_index<<<(c + 127) / 128, 128, 0, L.st>>>(
+                        (const unsigned long long*)(d + o_base), (const uint32_t*)(d + pl.o_grp),
+                        (const uint32_t*)(d + pl.o_rank), (const uint64_t*)(d + pl.o_plan), c, d_idx, mismatch_dev);
+                    SignArgs g{};
+                    g.sm = d + pl.o_out;
+                    g.sm_off = (const uint64_t*)(d + pl.o_soff);
+                    g.mlen = (const uint64_t*)(d + pl.o_len);
+                    g.msg = d + pl.o_in;
+                    g.msg_off = (const uint64_t*)(d + pl.o_off);
+                    g.idx = d_idx;
+                    g.key = (const uint32_t*)(d + pl.o_key);
+                    g.key_root = pl.table->mat.as<uint8_t>(0) + 2 * p.n;
+                    g.key_stride = 4 * p.n;
+                    g.tree_off = (const uint64_t*)(d + pl.o_toff);
+                    g.nodes = pool.as<uint8_t>(0);
+                    g.lens = L.w.lens.as<uint8_t>((size_t)c * p.d * pl.ops->len);
+                    g.count = c;
+                    g.index_bytes = p.index_bytes;
+                    g.sig_bytes = p.sig_bytes;
+                    g.tree_height = p.tree_height;
+                    g.d = p.d;
+                    pl.ops->sign_prep(g, pl.table->ctx.as<uint8_t>(0), L.st);
+                    pl.ops->sign_chains(g, pl.table->ctx.as<uint8_t>(0), L.st);
+                    groups_sign++;
+                }
             }
         }
         XB_CUDA(cudaEventRecord(L.done, L.st));
@@ -739,6 +787,16 @@ Launch xmss_b200_server::launch(Slot& s, std::vector<std::unique_ptr<Request>>& 
     s.admitted = std::max(s.admitted, est);
     s.any_sign = G != 0;
     s.launched = Clock::now();
+    s.lanes_used = nl;
+    s.trace = xmss_b200_batch_trace{};
+    s.trace.seq = batch_seq;
+    s.trace.requests = (uint32_t)reqs.size();
+    s.trace.plans = (uint32_t)nl;
+    s.trace.h2d_bytes = in_end;
+    s.trace.d2h_bytes = total - out_begin;
+    Clock::time_point oldest = s.launched;
+    for (auto& rp : reqs) oldest = std::min(oldest, rp->t0);
+    s.trace.queue_us = std::chrono::duration<double, std::micro>(s.launched - oldest).count();
     s.reqs = std::move(reqs);
     s.busy = true;
     std::lock_guard<std::mutex> lk(mu);
@@ -774,7 +832,26 @@ void xmss_b200_server::finish(Slot& s)
     });
     release(s);
     s.busy = false;
+    xmss_b200_batch_trace& tr = s.trace;
+    tr.done_us = std::chrono::duration<double, std::micro>(t0 - s.launched).count();
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, s.staged, s.done) == cudaSuccess) tr.gpu_us = 1e3 * ms;
+    double last_end = 0;
+    for (size_t i = 0; i < s.lanes_used; i++) {
+        const Lane& L = *s.lanes[i];
+        if (cudaEventElapsedTime(&ms, L.start, L.done) == cudaSuccess && 1e3 * ms > tr.lane_us) {
+            tr.lane_us = 1e3 * ms;
+            tr.slow_kind = L.kind;
+            tr.slow_oid = L.oid;
+        }
+        if (cudaEventElapsedTime(&ms, s.staged, L.start) == cudaSuccess) tr.start_skew_us = std::max(tr.start_skew_us, 1e3 * ms);
+        if (cudaEventElapsedTime(&ms, s.staged, L.done) == cudaSuccess) last_end = std::max(last_end, 1e3 * (double)ms);
+    }
+    tr.join_us = tr.gpu_us - last_end;
+    cudaGetLastError();  // clear a not-ready / invalid-handle status of the queries above
     std::lock_guard<std::mutex> lk(mu);
+    traces.push_back(tr);
+    if (traces.size() > 4096) traces.pop_front();
     stats.batch_us += std::chrono::duration<double, std::micro>(t0 - s.launched).count();
     stats.finish_us += std::chrono::duration<double, std::micro>(Clock::now() - t0).count();
     if (mismatch) fatal = "xmss_b200_server: device index counter differs from the plan";
@@ -825,8 +902,10 @@ void xmss_b200_server::run()
             const Clock::time_point t0 = Clock::now();
             res = launch(*free_slot, take, wait_pool);
             {
+                const double us = std::chrono::duration<double, std::micro>(Clock::now() - t0).count();
+                free_slot->trace.launch_us = us;
                 std::lock_guard<std::mutex> g(mu);
-                stats.launch_us += std::chrono::duration<double, std::micro>(Clock::now() - t0).count();
+                stats.launch_us += us;
             }
             if (res == Launch::kNothing) {  // refused while planning, or warm and cached
                 release(*free_slot);
@@ -963,13 +1042,16 @@ extern "C" int xmss_b200_server_create(const xmss_b200_server_config* cfg, xmss_
         for (uint32_t i = 0; i < c.slots; i++) {
             auto s = std::make_unique<Slot>();
             XB_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
-            XB_CUDA(cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming));
-            XB_CUDA(cudaEventCreateWithFlags(&s->staged, cudaEventDisableTiming));
+            XB_CUDA(cudaEventCreate(&s->done));
+            XB_CUDA(cudaEventCreate(&s->staged));
             XB_CUDA(cudaEventCreateWithFlags(&s->reserved, cudaEventDisableTiming));
             s->dev.order_on(s->st);
+            // staging for a full batch of long messages up front: growing
+            // pinned memory later takes tens of milliseconds of page pinning
+            const size_t stage = std::min<size_t>((size_t)c.max_batch << 16, 256ull << 20);
             s->stage.keep_old_blocks();
-            s->stage.get(64ull << 20);
-            s->dev.get(64ull << 20);
+            s->stage.get(stage);
+            s->dev.get(stage);
             srv->slots.push_back(std::move(s));
         }
         for (auto& sp : srv->slots) XB_CUDA(cudaStreamSynchronize(sp->st));
@@ -997,6 +1079,7 @@ extern "C" void xmss_b200_server_destroy(xmss_b200_server* srv)
     for (auto& s : srv->slots) {
         for (auto& ln : s->lanes) {
             cudaStreamSynchronize(ln->st);
+            cudaEventDestroy(ln->start);
             cudaEventDestroy(ln->done);
             cudaStreamDestroy(ln->st);
         }
@@ -1208,4 +1291,12 @@ extern "C" int xmss_b200_server_replay(xmss_b200_server* srv, const xmss_b200_tr
     submitter.join();
     if (elapsed_s) *elapsed_s = std::chrono::duration<double>(last - start).count();
     return 0;
+}
+
+extern "C" int xmss_b200_server_trace(xmss_b200_server* srv, xmss_b200_batch_trace* out, uint32_t max)
+{
+    std::lock_guard<std::mutex> g(srv->mu);
+    const size_t n = std::min<size_t>(max, srv->traces.size());
+    for (size_t i = 0; i < n; i++) out[i] = srv->traces[srv->traces.size() - n + i];
+    return (int)n;
 }

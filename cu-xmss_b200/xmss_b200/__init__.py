@@ -21,6 +21,10 @@ from typing import Sequence
 
 import numpy as np
 
+# 32 hardware work queues for the serving loop's streams (read by the CUDA
+# runtime when the process creates its first context; an existing setting wins)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 # XMSS_B200_LIB selects another build of the library (e.g. a tuning variant)
 LIB_PATH = os.environ.get("XMSS_B200_LIB") or os.path.join(HERE, "libxmss_b200.so")
@@ -134,6 +138,19 @@ class ServerStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchTrace(C.Structure):
+    """xmss_b200_batch_trace (include/xmss_b200.h)."""
+
+    _fields_ = [("seq", C.c_uint64), ("requests", C.c_uint32), ("plans", C.c_uint32), ("slow_kind", C.c_uint32),
+                ("slow_oid", C.c_uint32), ("queue_us", C.c_double), ("launch_us", C.c_double),
+                ("gpu_us", C.c_double), ("lane_us", C.c_double), ("done_us", C.c_double),
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64), ("start_skew_us", C.c_double),
+                ("join_us", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 # xmss_b200_trace_item as a numpy record (same layout as the C struct)
 TRACE_DTYPE = np.dtype([("t_us", "<f8"), ("kind", "<u4"), ("key_id", "<u4"), ("mt", "<i4"), ("reserved0", "<u4"),
                         ("in_ptr", "<u8"), ("inlen", "<u8"), ("sm_ptr", "<u8"), ("smlen_ptr", "<u8"),
@@ -152,6 +169,7 @@ lib.xmss_b200_server_submit_verify.argtypes = [_srvp, C.c_int, C.c_void_p, C.c_u
 lib.xmss_b200_server_submit_warm.argtypes = [_srvp, C.c_uint32, C.c_uint64]
 lib.xmss_b200_server_poll.argtypes = [_srvp, C.POINTER(Completion), C.c_uint32, C.c_uint32]
 lib.xmss_b200_server_stats_get.argtypes = [_srvp, C.POINTER(ServerStats)]
+lib.xmss_b200_server_trace.argtypes = [_srvp, C.POINTER(BatchTrace), C.c_uint32]
 lib.xmss_b200_server_replay.argtypes = [_srvp, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.POINTER(C.c_double)]
 
@@ -594,6 +612,12 @@ class Server:
         if r:
             raise GpuError(f"server failed: {last_error()}")
         return st.as_dict()
+
+    def batch_trace(self, max_items: int = 4096) -> list[dict]:
+        """The most recent batch records (xmss_b200_server_trace), oldest first."""
+        arr = (BatchTrace * max_items)()
+        n = lib.xmss_b200_server_trace(self._h, arr, max_items)
+        return [arr[i].as_dict() for i in range(n)]
 
     def replay(self, trace: np.ndarray):
         """xmss_b200_server_replay over a TRACE_DTYPE array (pointers inside must

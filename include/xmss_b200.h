@@ -223,6 +223,28 @@ int xmss_b200_server_poll(xmss_b200_server *srv, xmss_b200_completion *out, uint
 /* 0 ok, -3 when the dispatcher has failed (text in xmss_b200_last_error()). */
 int xmss_b200_server_stats_get(xmss_b200_server *srv, xmss_b200_server_stats *out);
 
+/* Per-batch trace: the server keeps the last 4096 batches.  Times in us;
+ * gpu_us spans the batch's first device operation to its last (CUDA events),
+ * lane_us is the slowest plan, identified by its operation (0 sign, 1 verify)
+ * and OID. */
+typedef struct {
+    uint64_t seq;
+    uint32_t requests, plans;
+    uint32_t slow_kind, slow_oid;
+    double queue_us;   /* oldest request: submission to launch */
+    double launch_us;  /* host planning, staging and launching */
+    double gpu_us;
+    double lane_us;
+    double done_us;    /* launch to completion seen by the dispatcher */
+    uint64_t h2d_bytes, d2h_bytes;
+    double start_skew_us;  /* latest lane start after the inputs landed */
+    double join_us;        /* batch end after the last lane ended */
+} xmss_b200_batch_trace;
+
+/* Copies up to max of the most recent batch records, oldest first; returns
+ * how many. */
+int xmss_b200_server_trace(xmss_b200_server *srv, xmss_b200_batch_trace *out, uint32_t max);
+
 /* Load generator: submits items (sorted by t_us) at their times from a
  * submitting thread while this thread polls, until all complete.  Latency is
  * measured from each item's scheduled time, so a submitter that falls behind
