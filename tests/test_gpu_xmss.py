@@ -2,6 +2,7 @@
 reference's own outputs (golden fixtures) and the CPU oracle."""
 import hashlib
 import os
+import zlib
 
 import numpy as np
 import pytest
@@ -271,3 +272,35 @@ def test_hmsg_block_edges_every_family(xb, oracle, golden):
         pkarr = np.frombuffer(oidb + pk, np.uint8)[None, :]
         st = xb.sign_open_batch(True, buf, off, ln, pkarr, np.zeros(len(variants), np.uint32))
         assert list(st) == expect, k["oid"]
+
+
+@pytest.mark.parametrize("name", ["XMSSMT-SHA2_40/8_256", "XMSSMT-SHA2_60/6_256", "XMSSMT-SHA2_60/12_256",
+                                  "XMSSMT-SHAKE_20/4_512", "XMSSMT-SHA2_20/4_192",
+                                  "XMSSMT-SHAKE256_60/12_192"])
+def test_remaining_mt_heights(xb, oracle, name):
+    """XMSS^MT heights and hash widths beyond the fixtures (8 and 12 layers,
+    60-bit indices above 2^32, SHAKE256 with n = 64, SHA-256/192): keypair,
+    signatures at seeded indices and verify equal the oracle's."""
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
+    oid = xb.xmssmt_str_to_oid(name)
+    p, po = xb.parse_oid(oid, True), oracle.params(oid, True)
+    seed = rng.bytes(3 * p.n)
+    r, pk, sk = xb.xmssmt_core_seed_keypair(p, seed)
+    pk_o, sk_o = oracle.seed_keypair(po, seed)
+    assert r == 0 and pk == pk_o and sk == sk_o
+    top = (1 << p.full_height) - 1
+    for idx in (int(rng.integers(0, min(top, 1 << 31))), int(rng.integers(0, min(top, 1 << 62)))):
+        m = rng.bytes(int(rng.integers(0, 500)))
+        skx = idx.to_bytes(p.index_bytes, "big") + sk[p.index_bytes:]
+        r, sk2, sm = xb.xmssmt_core_sign(p, skx, m)
+        # the oracle signs from its own threaded node arrays of each layer's subtree
+        ib, n, th = p.index_bytes, p.n, p.tree_height
+        trees = b"".join(oracle.tree_nodes(po, sk[ib:ib + n], sk[ib + 3 * n:ib + 4 * n], layer,
+                                           idx >> (th * (layer + 1)) if th * (layer + 1) < 64 else 0,
+                                           os.cpu_count()) for layer in range(p.d))
+        ro, sk2o, smo = oracle.sign(po, skx, m, trees=trees)
+        assert r == ro == 0 and sm == smo and sk2 == sk2o, (name, idx)
+        assert xb.xmssmt_core_sign_open(p, sm, pk) == (0, m)
+        bad = bytearray(sm)
+        bad[int(rng.integers(0, len(bad)))] ^= 1
+        assert xb.xmssmt_core_sign_open(p, bytes(bad), pk)[0] == -1
