@@ -9,6 +9,8 @@
 
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -476,6 +478,91 @@ extern "C" int xmss_b200_sign_open_batch(int mt, uint32_t count, const uint8_t* 
             return kBad;
         }
     return verify_host(p, count, sm, sm_off, smlen, pk + XMSS_OID_LEN, pks, npk, pk_index, status);
+}
+
+namespace {
+
+// Buffers of one caller stream for xmss_b200_sign_open_batch_async: scratch
+// and staging that grow stream-ordered on that stream, a second stream for
+// the split of large batches, and the end of the stream's last call.
+struct StreamCtx {
+    xb::Workspace w;
+    xb::DevBuf d;
+    xb::PinnedBuf h;
+    cudaEvent_t done = nullptr;
+    bool pending = false;
+};
+
+std::map<cudaStream_t, std::unique_ptr<StreamCtx>> g_stream_ctx;  // guarded by Engine::mu
+
+StreamCtx& stream_ctx(cudaStream_t st)
+{
+    auto& c = g_stream_ctx[st];
+    if (!c) {
+        auto n = std::make_unique<StreamCtx>();
+        n->w.order_on(st);
+        n->d.order_on(st);
+        n->h.keep_old_blocks();
+        XB_CUDA(cudaStreamCreateWithFlags(&n->w.split_st, cudaStreamNonBlocking));
+        XB_CUDA(cudaEventCreateWithFlags(&n->w.split_fork, cudaEventDisableTiming));
+        XB_CUDA(cudaEventCreateWithFlags(&n->w.split_join, cudaEventDisableTiming));
+        XB_CUDA(cudaEventCreateWithFlags(&n->done, cudaEventDisableTiming));
+        c = std::move(n);
+    }
+    return *c;
+}
+
+}  // namespace
+
+extern "C" int xmss_b200_sign_open_batch_async(int mt, uint32_t count, const uint8_t* sm, const uint64_t* sm_off,
+                                               const uint64_t* smlen, const uint8_t* pk, uint32_t npk,
+                                               const uint32_t* pk_index, int* status, void* stream)
+{
+    if (!npk) return count ? kBad : kOk;
+    const uint32_t oid = (uint32_t)be_read(pk, XMSS_OID_LEN);
+    xmss_params p;
+    if (parse(&p, oid, mt)) return kBad;
+    const size_t pks = XMSS_OID_LEN + 2 * p.n;
+    for (uint32_t k = 1; k < npk; k++)
+        if ((uint32_t)be_read(pk + k * pks, XMSS_OID_LEN) != oid) {
+            g_err = "xmss_b200_sign_open_batch_async: public keys of different OIDs";
+            return kBad;
+        }
+    if (!count) return kOk;
+    return guarded([&](Engine& e) {
+        const xb::FamilyOps* ops = xb::ops_for(p);
+        cudaStream_t st = (cudaStream_t)stream;
+        XB_CUDA(cudaSetDevice(e.device()));
+        StreamCtx& c = stream_ctx(st);
+        // the stream's previous call must be past its staging
+        if (c.pending) XB_CUDA(cudaEventSynchronize(c.done));
+        uint64_t raw = 0;
+        for (uint32_t i = 0; i < count; i++) raw = std::max(raw, sm_off[i] + smlen[i]);
+        const uint64_t span = (raw + 15) & ~15ull;
+        const size_t n2 = 2 * (size_t)p.n;
+        const size_t o_off = span, o_len = o_off + count * 8, o_pk = o_len + count * 8,
+                     o_idx = o_pk + ((npk * n2 + 15) & ~(size_t)15), o_st = o_idx + ((count * 4 + 15) & ~(size_t)15),
+                     total = o_st + count * 4;
+        uint8_t* h = c.h.as<uint8_t>(total - o_off);
+        memcpy(h, sm_off, count * 8);
+        memcpy(h + (o_len - o_off), smlen, count * 8);
+        for (uint32_t k = 0; k < npk; k++) memcpy(h + (o_pk - o_off) + k * n2, pk + XMSS_OID_LEN + k * pks, n2);
+        uint32_t* hi = (uint32_t*)(h + (o_idx - o_off));
+        for (uint32_t i = 0; i < count; i++) {
+            hi[i] = pk_index ? pk_index[i] : i;
+            if (hi[i] >= npk) throw std::invalid_argument("pk_index out of range");
+        }
+        uint8_t* d = c.d.as<uint8_t>(total);
+        if (raw) XB_CUDA(cudaMemcpyAsync(d, sm, raw, cudaMemcpyHostToDevice, st));
+        XB_CUDA(cudaMemcpyAsync(d + o_off, h, o_st - o_off, cudaMemcpyHostToDevice, st));
+        e.verify(ops, p, count, d, (const uint64_t*)(d + o_off), (const uint64_t*)(d + o_len), d + o_pk, npk,
+                 (const uint32_t*)(d + o_idx), (int*)(d + o_st), st, c.w, true);
+        XB_CUDA(cudaMemcpyAsync(status, d + o_st, count * 4, cudaMemcpyDeviceToHost, st));
+        XB_CUDA(cudaGetLastError());
+        XB_CUDA(cudaEventRecord(c.done, st));
+        c.pending = true;
+        return kOk;
+    });
 }
 
 extern "C" int xmss_b200_sign_open_device(uint32_t oid, int mt, uint32_t count, const uint8_t* d_sm,

@@ -389,7 +389,9 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
     // H_msg is short start their chains at once while the long messages are
     // still being hashed (H_msg is a serial chain of compressions).  The
     // profiling pass keeps one sequence so each kernel's time is its own.
-    if (!allow_split || count < kSplitMin || profiling) {
+    cudaStream_t aux = own ? aux_ : w.split_st;
+    cudaEvent_t fork = own ? fork_ : w.split_fork, join = own ? join_ : w.split_join;
+    if (!allow_split || count < kSplitMin || profiling || !aux) {
         verify_sequence(ops, p, v, ctx, st, own);
         return;
     }
@@ -404,12 +406,12 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
     b.sel_n = n2 + 1;
     b.hist = hist + 32 * p.d;
     b.list = w.list2.as<uint32_t>((size_t)count * len);  // each group has its own chain list
-    XB_CUDA(cudaEventRecord(fork_, st));
-    XB_CUDA(cudaStreamWaitEvent(aux_, fork_, 0));
-    verify_sequence(ops, p, b, ctx, aux_, own);
+    XB_CUDA(cudaEventRecord(fork, st));
+    XB_CUDA(cudaStreamWaitEvent(aux, fork, 0));
+    verify_sequence(ops, p, b, ctx, aux, own);
     verify_sequence(ops, p, a, ctx, st, own);
-    XB_CUDA(cudaEventRecord(join_, aux_));
-    XB_CUDA(cudaStreamWaitEvent(st, join_, 0));
+    XB_CUDA(cudaEventRecord(join, aux));
+    XB_CUDA(cudaStreamWaitEvent(st, join, 0));
 }
 
 void Engine::last_verify_work(unsigned long long out[3])

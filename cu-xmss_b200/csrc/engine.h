@@ -102,6 +102,10 @@ struct Workspace {
     DevBuf work;  // verify work counters of non-engine workspaces
     PinnedBuf h_jobs;
     void order_on(cudaStream_t st);  // every buffer grows stream-ordered on st
+    // Second stream of large verify batches (two groups split by H_msg
+    // length) for workspaces outside the engine; none: no split.
+    cudaStream_t split_st = nullptr;
+    cudaEvent_t split_fork = nullptr, split_join = nullptr;
 };
 
 class Engine {

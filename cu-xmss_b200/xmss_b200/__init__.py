@@ -106,6 +106,8 @@ lib.xmss_b200_sign_open_batch.argtypes = [C.c_int, C.c_uint32, _u8p, _u64p, _u64
 lib.xmss_b200_sign_open_device.argtypes = [C.c_uint32, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
                                            C.c_void_p]
+lib.xmss_b200_sign_open_batch_async.argtypes = [C.c_int, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
 lib.xmss_b200_sign_batch.argtypes = [C.c_int, C.c_uint32, _u8p, _u8p, _u64p, _u64p, _u8p, _u64p,
                                      _u64p, _intp]
 lib.xmss_b200_core_hash_batch.argtypes = [C.c_uint, C.c_uint, C.c_uint32, _u8p, _u64p, _u64p, _u8p]
@@ -394,6 +396,23 @@ def sign_open_batch(mt: bool, sm: np.ndarray, sm_off: np.ndarray, smlen: np.ndar
     if r:
         raise ValueError(f"sign_open_batch returned {r}: {last_error()}")
     return status
+
+
+def sign_open_batch_async(mt: bool, sm: np.ndarray, sm_off: np.ndarray, smlen: np.ndarray, pk: np.ndarray,
+                          pk_index: np.ndarray, status: np.ndarray, stream: int) -> None:
+    """xmss_b200_sign_open_batch_async: enqueue on `stream` and return.  sm
+    and status should be pinned (e.g. torch pin_memory) and stay alive and
+    untouched until the stream has passed the call."""
+    for a, t in ((sm, np.uint8), (sm_off, np.uint64), (smlen, np.uint64), (pk, np.uint8), (pk_index, np.uint32),
+                 (status, np.int32)):
+        if a.dtype != t or not a.flags.c_contiguous:
+            raise TypeError("sign_open_batch_async wants contiguous arrays of the documented dtypes")
+    r = _check(lib.xmss_b200_sign_open_batch_async(int(mt), len(sm_off), sm.ctypes.data, sm_off.ctypes.data,
+                                                   smlen.ctypes.data, pk.ctypes.data, pk.shape[0],
+                                                   pk_index.ctypes.data, status.ctypes.data, stream),
+               "sign_open_batch_async")
+    if r:
+        raise ValueError(f"sign_open_batch_async returned {r}: {last_error()}")
 
 
 def sign_batch(mt: bool, sk: np.ndarray, msgs: Sequence[bytes]):

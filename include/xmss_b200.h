@@ -69,6 +69,21 @@ int xmss_b200_sign_open_device(uint32_t oid, int mt, uint32_t count, const uint8
                                const uint8_t *d_pk, uint32_t npk, const uint32_t *d_pk_index,
                                int *d_status, void *stream);
 
+/* Pipelined form of xmss_b200_sign_open_batch: enqueues the copy of the
+ * signed messages from the caller's memory, the verify, and the copy of the
+ * statuses into `status` on `stream` (cudaStream_t as void*) and returns.
+ * sm and status should be pinned host memory (pageable memory makes the
+ * copies synchronous); they must stay untouched until the stream has
+ * passed this call (cudaStreamSynchronize or an event).  sm_off, smlen, pk
+ * and pk_index are read before the call returns.  Each stream has its own
+ * device buffers, so calls on two or more streams overlap one batch's
+ * copies with another's kernels; a call waits for the previous call on the
+ * same stream to finish first.  No reference counterpart beyond the
+ * xmss[mt]_sign_open calls it batches (xmss.c:45-60, 95-109). */
+int xmss_b200_sign_open_batch_async(int mt, uint32_t count, const uint8_t *sm, const uint64_t *sm_off,
+                                    const uint64_t *smlen, const uint8_t *pk, uint32_t npk,
+                                    const uint32_t *pk_index, int *status, void *stream);
+
 /* Batched xmss[mt]_sign (xmss.c:28-43, 78-93).  Request i signs
  * msgs[m_off[i] .. + mlen[i]) with sk i (sk: count x (4 + sk_bytes),
  * OID-prefixed, one OID), advancing that sk in place exactly as

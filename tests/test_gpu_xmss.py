@@ -304,3 +304,42 @@ def test_remaining_mt_heights(xb, oracle, name):
         bad = bytearray(sm)
         bad[int(rng.integers(0, len(bad)))] ^= 1
         assert xb.xmssmt_core_sign_open(p, bytes(bad), pk)[0] == -1
+
+
+def test_sign_open_batch_async_two_streams(xb, oracle):
+    """The pipelined host-buffer verify (xmss_b200_sign_open_batch_async)
+    gives the blocking call's statuses, with calls in flight on two streams
+    at once over the same pinned inputs, including the split path of large
+    batches."""
+    import torch
+
+    rng = np.random.default_rng(61)
+    keys, count = 3, 1500
+    seeds = np.frombuffer(rng.bytes(keys * 96), np.uint8).reshape(keys, 96)
+    pks, sks = xb.keypair_batch(1, False, seeds)
+    keyix = rng.integers(0, keys, count).astype(np.uint32)
+    rows = np.array(sks[keyix])
+    idx = rng.integers(0, 1024, count)
+    for i in range(count):
+        rows[i, 4:8] = np.frombuffer(int(idx[i]).to_bytes(4, "big"), np.uint8)
+    msgs = [rng.bytes(int(L)) for L in np.exp(rng.uniform(0, np.log(5000), count)).astype(int)]
+    ret, sms = xb.sign_batch(False, rows, msgs)
+    sms = [bytearray(s) for s in sms]
+    for i in range(0, count, 7):
+        sms[i][int(rng.integers(0, len(sms[i])))] ^= 1
+    buf, off, ln = xb.pack([bytes(s) for s in sms], align=16)
+    want = xb.sign_open_batch(False, buf, off, ln, pks, keyix)
+    assert (want[::7] == -1).sum() >= count // 7 - 3
+    h_sm = torch.from_numpy(buf).pin_memory().numpy()
+    outs = [torch.full((count,), 7, dtype=torch.int32).pin_memory().numpy() for _ in range(4)]
+    streams = [torch.cuda.Stream() for _ in range(2)]
+    sub = slice(0, 300)
+    for i, o in enumerate(outs):
+        if i < 2:
+            xb.sign_open_batch_async(False, h_sm, off, ln, pks, keyix, o, streams[i % 2].cuda_stream)
+        else:  # a small batch (no split) on the same streams
+            xb.sign_open_batch_async(False, h_sm, np.ascontiguousarray(off[sub]), np.ascontiguousarray(ln[sub]),
+                                     pks, np.ascontiguousarray(keyix[sub]), o, streams[i % 2].cuda_stream)
+    torch.cuda.synchronize()
+    assert (outs[0] == want).all() and (outs[1] == want).all()
+    assert (outs[2][:300] == want[:300]).all() and (outs[3][:300] == want[:300]).all()
