@@ -108,6 +108,10 @@ lib.xmss_b200_sign_open_device.argtypes = [C.c_uint32, C.c_int, C.c_uint32, C.c_
                                            C.c_void_p]
 lib.xmss_b200_sign_open_batch_async.argtypes = [C.c_int, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
                                                 C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+lib.xmss_b200_bds_sk_bytes.argtypes = [C.c_uint32, C.c_int]
+lib.xmss_b200_bds_sk_bytes.restype = C.c_ulonglong
+lib.xmss_b200_sk_from_bds.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+lib.xmss_b200_sk_to_bds.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
 lib.xmss_b200_sign_batch.argtypes = [C.c_int, C.c_uint32, _u8p, _u8p, _u64p, _u64p, _u8p, _u64p,
                                      _u64p, _intp]
 lib.xmss_b200_core_hash_batch.argtypes = [C.c_uint, C.c_uint, C.c_uint32, _u8p, _u64p, _u64p, _u8p]
@@ -452,6 +456,32 @@ def sign_batch_packed(mt: bool, sk: np.ndarray, mbuf: np.ndarray, moff: np.ndarr
                                         _np_ptr(smlen, C.c_uint64), _np_ptr(ret, C.c_int)), "sign_batch")
     if r:
         raise ValueError(f"sign_batch returned {r}: {last_error()}")
+
+
+def bds_sk_bytes(oid: int, mt: bool) -> int:
+    """Size of the reference's BDS ("fast") sk without the OID."""
+    return int(lib.xmss_b200_bds_sk_bytes(oid, int(mt)))
+
+
+def sk_from_bds(mt: bool, bds_sk: bytes) -> bytes:
+    """The plain OID-prefixed sk inside a BDS sk (xmss_b200_sk_from_bds)."""
+    oid = int.from_bytes(bytes(bds_sk[:4]), "big")
+    out = _buf(XMSS_OID_LEN + parse_oid(oid, mt).sk_bytes)
+    r = lib.xmss_b200_sk_from_bds(int(mt), _buf(bds_sk), out)
+    if r:
+        raise ValueError(f"sk_from_bds returned {r}")
+    return bytes(out)
+
+
+def sk_to_bds(mt: bool, sk: bytes) -> bytes:
+    """The BDS sk the reference's fast build holds at this sk's index
+    (xmss_b200_sk_to_bds)."""
+    oid = int.from_bytes(bytes(sk[:4]), "big")
+    out = _buf(XMSS_OID_LEN + bds_sk_bytes(oid, mt))
+    r = _check(lib.xmss_b200_sk_to_bds(int(mt), _buf(sk), out), "sk_to_bds")
+    if r:
+        raise ValueError(f"sk_to_bds returned {r}: {last_error()}")
+    return bytes(out)
 
 
 def core_hash_batch(func: int, n: int, msgs: Sequence[bytes]) -> list[bytes]:

@@ -282,6 +282,30 @@ typedef struct {
 int xmss_b200_server_replay(xmss_b200_server *srv, const xmss_b200_trace_item *items, uint32_t count, int *ret,
                             double *latency_us, uint64_t *index, double *elapsed_s);
 
+/* ---------------------------------------------------------------------------
+ * BDS ("fast") secret keys, as the reference's xmss_core_fast.c builds keep
+ * them (xmss_core_fast.c:14-148, 635-653): the plain sk followed by the
+ * authentication-path traversal state of 2d - 1 trees and, for XMSS^MT, the
+ * WOTS signatures of the lower roots.  Keys are OID-prefixed here.
+ * --------------------------------------------------------------------------- */
+
+/* Size of a BDS sk of this parameter set without the OID (0: unknown). */
+unsigned long long xmss_b200_bds_sk_bytes(uint32_t oid, int mt);
+
+/* The plain sk (what xmss[mt]_keypair writes) inside a BDS sk: its index,
+ * seeds, root and PUB_SEED.  0 ok, -1 unknown OID. */
+int xmss_b200_sk_from_bds(int mt, const uint8_t *bds_sk, uint8_t *sk);
+
+/* The BDS sk the reference's fast build holds at this plain sk's index:
+ * the traversal of keygen and of every signature below the index is
+ * replayed on the host (its hashes looked up in subtrees built on the GPU),
+ * so the time grows with the index; indices above 2^24 return -1.  Fields
+ * the reference never writes (it leaves the caller's buffer in them) are
+ * zero; a wiped key stays wiped.  At the last index (2^h - 1) the cached
+ * WOTS signatures are those of this library's sign at that index, which the
+ * reference never reads (it wipes the key before signing). */
+int xmss_b200_sk_to_bds(int mt, const uint8_t *sk, uint8_t *bds_sk);
+
 /* Compression-rate probe (the roofline denominator): `blocks` x 128 threads
  * each run `iters` dependent SHA-256 compressions (kind 0) or Keccak-f[1600]
  * permutations (kind 1) in registers, on `stream`.  d_sink: blocks x 128
