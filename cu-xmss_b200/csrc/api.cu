@@ -486,6 +486,7 @@ namespace {
 // and staging that grow stream-ordered on that stream, a second stream for
 // the split of large batches, and the end of the stream's last call.
 struct StreamCtx {
+    xb::SplitStreams split;
     xb::Workspace w;
     xb::DevBuf d;
     xb::PinnedBuf h;
@@ -503,9 +504,8 @@ StreamCtx& stream_ctx(cudaStream_t st)
         n->w.order_on(st);
         n->d.order_on(st);
         n->h.keep_old_blocks();
-        XB_CUDA(cudaStreamCreateWithFlags(&n->w.split_st, cudaStreamNonBlocking));
-        XB_CUDA(cudaEventCreateWithFlags(&n->w.split_fork, cudaEventDisableTiming));
-        XB_CUDA(cudaEventCreateWithFlags(&n->w.split_join, cudaEventDisableTiming));
+        n->split.create();
+        n->w.split = &n->split;
         XB_CUDA(cudaEventCreateWithFlags(&n->done, cudaEventDisableTiming));
         c = std::move(n);
     }

@@ -94,6 +94,14 @@ class PinnedBuf {
     std::vector<void*> retired_;
 };
 
+// Second stream of a split verify batch (the long-H_msg group runs there
+// while the short group runs on the caller's stream) and its fork / join.
+struct SplitStreams {
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    void create();
+};
+
 // Scratch of one in-flight launch sequence.  The engine owns one for its
 // own entry points; the server gives each of its batch slots one, so
 // batches on different streams never share intermediate buffers.
@@ -102,10 +110,9 @@ struct Workspace {
     DevBuf work;  // verify work counters of non-engine workspaces
     PinnedBuf h_jobs;
     void order_on(cudaStream_t st);  // every buffer grows stream-ordered on st
-    // Second stream of large verify batches (two groups split by H_msg
-    // length) for workspaces outside the engine; none: no split.
-    cudaStream_t split_st = nullptr;
-    cudaEvent_t split_fork = nullptr, split_join = nullptr;
+    // Streams of large verify batches (two groups split by H_msg length)
+    // for workspaces outside the engine; none: no split.
+    SplitStreams* split = nullptr;
 };
 
 class Engine {
@@ -200,8 +207,7 @@ class Engine {
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
     cudaEvent_t done_ = nullptr;
-    cudaStream_t aux_ = nullptr;  // second stream of split verify batches
-    cudaEvent_t fork_ = nullptr, join_ = nullptr;
+    SplitStreams split_;  // streams of the engine's own split verify batches
     bool have_done_ = false;
     Workspace ws_;  // scratch of the engine's own entry points
     DevBuf s_work_;
