@@ -10,7 +10,10 @@ own batched keygen / sign (untimed) and the accept bitmap is checked.
 
 value      verifies/s with inputs resident in HBM, CUDA events around each
            step on the launching stream, L2 flushed between steps (the input
-           is 14 MB, smaller than L2), max over ranks (replicas, weak scaling)
+           is 14 MB, smaller than L2), max over ranks (replicas, weak scaling);
+           the steps run once as launches of xmss_b200_sign_open_device and
+           once as replays of its CUDA graph (xmss_b200_verify_graph_*), and
+           the faster is the value (both are reported in config)
 e2e        the same through the host-buffer C-ABI from pinned host memory,
            every step's copies included: xmss_b200_sign_open_batch_async on
            two streams in turn (one step's copies overlap the other's
@@ -227,7 +230,35 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if world > 1:
         dist.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    t_ms = max_over_ranks(float(sum(step_ms)), world, dev)
+    t_ms_stream = max_over_ranks(float(sum(step_ms)), world, dev)
+
+    # ---- the same steps replayed from a CUDA graph of the launch sequence ----
+    graph = xb.VerifyGraph(OID, False, NUM_SIGS, d_sm.data_ptr(), d_off.data_ptr(), d_len.data_ptr(),
+                           d_pk.data_ptr(), NUM_KEYS, d_kix.data_ptr(), d_status.data_ptr())
+    for _ in range(args.warmup):
+        flush.zero_()
+        graph.launch(sh)
+    torch.cuda.synchronize()
+    d_status.fill_(7)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as gclocks:
+        for i in range(args.steps):
+            flush.zero_()
+            starts[i].record(stream)
+            graph.launch(sh)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    correct = correct and bool((d_status.cpu().numpy() == w["expect"]).all())
+    graph.close()
+    t_ms_graph = max_over_ranks(float(sum(s.elapsed_time(e) for s, e in zip(starts, ends))), world, dev)
+    launch_mode = "cuda_graph" if t_ms_graph < t_ms_stream else "stream"
+    if launch_mode == "cuda_graph":
+        clocks = gclocks
+    t_ms = min(t_ms_graph, t_ms_stream)
     value = replica_rate(NUM_SIGS, world, args.steps, t_ms / 1e3)
 
     # ---- per-kernel timing (separate pass; profiling serialises calls) ----
@@ -342,7 +373,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "config": {"workload": "batched verify, XMSS-SHA2_10_256", "oid": OID, "signatures": NUM_SIGS,
                    "keys": NUM_KEYS, "mlen": "log-uniform 32..4096 B", "mean_mlen": w["mean_mlen"],
                    "bitflip_fraction": 0.1, "parallelism": f"replicas x{world}",
-                   "l2": "flushed between steps (512 MB write; inputs 14 MB < 126 MB L2)"},
+                   "l2": "flushed between steps (512 MB write; inputs 14 MB < 126 MB L2)",
+                   "launch": launch_mode,
+                   "ms_per_step_stream_launches": t_ms_stream / args.steps,
+                   "ms_per_step_cuda_graph": t_ms_graph / args.steps},
         "correct": correct,
         "e2e": {"value": e2e_value, "unit": "verifies/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "blocking_call_verifies_per_s": NUM_SIGS / blocking_s,

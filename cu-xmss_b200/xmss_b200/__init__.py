@@ -112,6 +112,11 @@ lib.xmss_b200_bds_sk_bytes.argtypes = [C.c_uint32, C.c_int]
 lib.xmss_b200_bds_sk_bytes.restype = C.c_ulonglong
 lib.xmss_b200_sk_from_bds.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
 lib.xmss_b200_sk_to_bds.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+lib.xmss_b200_verify_graph_create.argtypes = [C.c_uint32, C.c_int, C.c_uint32] + [C.c_void_p] * 4 + [
+    C.c_uint32, C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]
+lib.xmss_b200_verify_graph_launch.argtypes = [C.c_void_p, C.c_void_p]
+lib.xmss_b200_verify_graph_destroy.argtypes = [C.c_void_p]
+lib.xmss_b200_verify_graph_destroy.restype = None
 lib.xmss_b200_sign_batch.argtypes = [C.c_int, C.c_uint32, _u8p, _u8p, _u64p, _u64p, _u8p, _u64p,
                                      _u64p, _intp]
 lib.xmss_b200_core_hash_batch.argtypes = [C.c_uint, C.c_uint, C.c_uint32, _u8p, _u64p, _u64p, _u8p]
@@ -682,3 +687,31 @@ class Server:
         if r:
             raise ValueError(f"server_replay returned {r}")
         return ret, lat, idx, el.value
+
+
+class VerifyGraph:
+    """xmss_b200_verify_graph_*: a device verify of fixed shape captured in a
+    CUDA graph (device pointers as ints)."""
+
+    def __init__(self, oid: int, mt: bool, count: int, d_sm: int, d_sm_off: int, d_smlen: int, d_pk: int, npk: int,
+                 d_pk_index: int, d_status: int):
+        h = C.c_void_p()
+        r = _check(lib.xmss_b200_verify_graph_create(oid, int(mt), count, d_sm, d_sm_off, d_smlen, d_pk, npk,
+                                                     d_pk_index, d_status, C.byref(h)), "verify_graph_create")
+        if r:
+            raise ValueError(f"verify_graph_create returned {r}: {last_error()}")
+        self._h = h
+
+    def launch(self, stream: int = 0) -> None:
+        _check(lib.xmss_b200_verify_graph_launch(self._h, stream), "verify_graph_launch")
+
+    def close(self) -> None:
+        if self._h:
+            lib.xmss_b200_verify_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -84,6 +84,21 @@ int xmss_b200_sign_open_batch_async(int mt, uint32_t count, const uint8_t *sm, c
                                     const uint64_t *smlen, const uint8_t *pk, uint32_t npk,
                                     const uint32_t *pk_index, int *status, void *stream);
 
+/* CUDA-graph form of xmss_b200_sign_open_device for batches of a fixed
+ * shape at fixed device addresses (a verifier that refills the same
+ * buffers): create runs the verify once (sizing the graph's own scratch)
+ * and captures its whole launch sequence; launch replays it with one call,
+ * reading whatever the buffers hold then.  Launches of one graph must not
+ * overlap each other; destroy waits for the device. */
+typedef struct xmss_b200_verify_graph xmss_b200_verify_graph;
+
+int xmss_b200_verify_graph_create(uint32_t oid, int mt, uint32_t count, const uint8_t *d_sm,
+                                  const uint64_t *d_sm_off, const uint64_t *d_smlen, const uint8_t *d_pk,
+                                  uint32_t npk, const uint32_t *d_pk_index, int *d_status,
+                                  xmss_b200_verify_graph **out);
+int xmss_b200_verify_graph_launch(xmss_b200_verify_graph *g, void *stream);
+void xmss_b200_verify_graph_destroy(xmss_b200_verify_graph *g);
+
 /* Batched xmss[mt]_sign (xmss.c:28-43, 78-93).  Request i signs
  * msgs[m_off[i] .. + mlen[i]) with sk i (sk: count x (4 + sk_bytes),
  * OID-prefixed, one OID), advancing that sk in place exactly as

@@ -51,3 +51,26 @@ def test_unknown_oid_rejected_before_gpu(xb):
     """OID parsing happens on the host: unknown OIDs return -1 like xmss.c."""
     r, _, _ = xb.xmss_keypair(0x99)
     assert r == -1
+
+
+def test_binding_argtypes_match_headers(xb):
+    """Every binding that sets argtypes passes as many arguments as the
+    header declares (a miscount only shows when the GPU call is made)."""
+    import os
+    import re
+
+    decls = {}
+    for f in sorted(os.listdir(xb.INCLUDE_DIR)):
+        if f.endswith(".h"):
+            text = re.sub(r"/\*.*?\*/", "", open(os.path.join(xb.INCLUDE_DIR, f)).read(), flags=re.S)
+            for name, args in re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(([^;{()]*(?:\([^()]*\)[^;{()]*)*)\)\s*;",
+                                         text):
+                args = re.sub(r"\([^()]*\)", "P", args).strip()  # function-pointer groups
+                decls[name] = 0 if args in ("", "void") else args.count(",") + 1
+    checked = 0
+    for name, nargs in decls.items():
+        fn = getattr(xb.lib, name, None)
+        if fn is not None and fn.argtypes is not None:
+            assert len(fn.argtypes) == nargs, (name, len(fn.argtypes), nargs)
+            checked += 1
+    assert checked >= 25

@@ -343,3 +343,60 @@ def test_sign_open_batch_async_two_streams(xb, oracle):
     torch.cuda.synchronize()
     assert (outs[0] == want).all() and (outs[1] == want).all()
     assert (outs[2][:300] == want[:300]).all() and (outs[3][:300] == want[:300]).all()
+
+
+@pytest.mark.parametrize("count", [300, 1100])
+def test_verify_graph_replays(xb, count):
+    """A verify captured in a CUDA graph (xmss_b200_verify_graph_*) gives the
+    statuses of the plain device call, and replays read the buffers' current
+    contents (refilled with other signatures between launches); 1,100
+    signatures take the two-stream split inside the graph."""
+    import torch
+
+    rng = np.random.default_rng(83 + count)
+    keys = 4
+    seeds = np.frombuffer(rng.bytes(keys * 96), np.uint8).reshape(keys, 96)
+    pks, sks = xb.keypair_batch(1, False, seeds)
+    batches = []
+    for _ in range(2):
+        keyix = rng.integers(0, keys, count).astype(np.uint32)
+        rows = np.array(sks[keyix])
+        idx = rng.integers(0, 1023, count)
+        for i in range(count):
+            rows[i, 4:8] = np.frombuffer(int(idx[i]).to_bytes(4, "big"), np.uint8)
+        msgs = [rng.bytes(int(L)) for L in np.exp(rng.uniform(0, np.log(3000), count)).astype(int)]
+        _, sms = xb.sign_batch(False, rows, msgs)
+        sms = [bytearray(s) for s in sms]
+        for i in range(int(rng.integers(0, 5)), count, 5):
+            sms[i][int(rng.integers(0, len(sms[i])))] ^= 1
+        buf, off, ln = xb.pack([bytes(s) for s in sms], align=16)
+        want = xb.sign_open_batch(False, buf, off, ln, pks, keyix)
+        batches.append((buf, off, ln, keyix, want))
+    cap = max(len(b[0]) for b in batches)
+    dev = torch.device("cuda", 0)
+    d_sm = torch.zeros(cap, dtype=torch.uint8, device=dev)
+    d_off = torch.zeros(count, dtype=torch.int64, device=dev)
+    d_len = torch.zeros(count, dtype=torch.int64, device=dev)
+    d_kix = torch.zeros(count, dtype=torch.int32, device=dev)
+    d_pk = torch.from_numpy(np.ascontiguousarray(pks[:, 4:])).to(dev)
+    d_st = torch.full((count,), 7, dtype=torch.int32, device=dev)
+
+    def load(b):
+        buf, off, ln, keyix, _ = b
+        d_sm[:len(buf)].copy_(torch.from_numpy(buf))
+        d_off.copy_(torch.from_numpy(off.astype(np.int64)))
+        d_len.copy_(torch.from_numpy(ln.astype(np.int64)))
+        d_kix.copy_(torch.from_numpy(keyix.astype(np.int32)))
+        torch.cuda.synchronize()
+
+    load(batches[0])
+    g = xb.VerifyGraph(1, False, count, d_sm.data_ptr(), d_off.data_ptr(), d_len.data_ptr(), d_pk.data_ptr(), keys,
+                       d_kix.data_ptr(), d_st.data_ptr())
+    for rep in range(3):
+        b = batches[rep % 2]
+        load(b)
+        d_st.fill_(7)
+        g.launch(torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        assert (d_st.cpu().numpy() == b[4]).all(), rep
+    g.close()
