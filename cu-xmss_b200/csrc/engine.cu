@@ -397,14 +397,15 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
     // still being hashed (H_msg is a serial chain of compressions).  The
     // profiling pass keeps one sequence so each kernel's time is its own.
     SplitStreams* ss = own ? &split_ : w.split;
-    if (!allow_split || count < kSplitMin || profiling || !ss) {
+    const Tuning& tn = tuning_for(ops->func, ops->n);
+    if (!allow_split || count < tn.split_min || profiling || !ss) {
         verify_sequence(ops, p, v, ctx, st, own);
         return;
     }
     uint32_t* n2 = hist + 2 * 32 * p.d;
     uint32_t* sel_short = list + (size_t)count * len;
     uint32_t* sel_long = sel_short + count;
-    ops->verify_partition(v, kShortHmsgBlocks, sel_short, sel_long, n2, st);
+    ops->verify_partition(v, tn.short_hmsg_blocks, sel_short, sel_long, n2, st);
     VerifyArgs a = v, b = v;
     a.sel = sel_short;
     a.sel_n = n2;

@@ -185,10 +185,8 @@ class Engine {
     // v.sel is null), on one stream.
     void verify_sequence(const FamilyOps* ops, const xmss_params& p, const VerifyArgs& v, const void* ctx,
                          cudaStream_t st, bool marks = true);
-    // Batches of at least kSplitMin signatures are verified as two groups
-    // split at kShortHmsgBlocks hash blocks of H_msg.
-    static constexpr uint32_t kSplitMin = 1024;
-    static constexpr uint32_t kShortHmsgBlocks = 16;
+    // Batches of at least Tuning::split_min signatures are verified as two
+    // groups split at Tuning::short_hmsg_blocks hash blocks of H_msg.
 
     // Work counters of the last verify (see xmss_b200_last_verify_work).
     void last_verify_work(unsigned long long out[3]);

@@ -9,9 +9,9 @@ namespace xb {
 
 constexpr int kBlock = 128;
 
-inline unsigned grid_for(uint64_t items)
+inline unsigned grid_for(uint64_t items, unsigned block = kBlock)
 {
-    return (unsigned)((items + kBlock - 1) / kBlock);
+    return (unsigned)((items + block - 1) / block);
 }
 
 // F runs every kernel except the chain kernels, which run FT (the same
@@ -19,6 +19,8 @@ inline unsigned grid_for(uint64_t items)
 template <class F, class FT = F>
 struct Launch {
     using Ctx = typename F::Ctx;
+    static inline unsigned s_func = 0;  // set by table()
+    static const Tuning& tune() { return tuning_for(s_func, (unsigned)F::N); }
     static_assert(sizeof(typename FT::Ctx) == sizeof(Ctx), "chain family must share the key context");
 
     static void make_ctx(const uint8_t* pub, uint32_t pub_stride, const uint8_t* sks, uint32_t sks_stride,
@@ -33,8 +35,9 @@ struct Launch {
     {
         const uint64_t items = nslots * F::LEN;
         if (!items) return;
+        const unsigned b = tune().keygen_chain_block;
         k_keygen_chains<FT>
-            <<<grid_for(items), kBlock, 0, st>>>(jobs, h, slot0, nslots, (const typename FT::Ctx*)ctx, wpk, refs);
+            <<<grid_for(items, b), b, 0, st>>>(jobs, h, slot0, nslots, (const typename FT::Ctx*)ctx, wpk, refs);
     }
     static void ltree_level(const LeafRef* refs, uint32_t nslots, int level, int cnt_in, const uint8_t* src,
                             uint32_t src_stride, uint8_t* dst, uint32_t dst_stride, uint8_t* leaf_out,
@@ -42,15 +45,17 @@ struct Launch {
     {
         const uint64_t items = (uint64_t)nslots * ((cnt_in + 1) / 2);
         if (!items) return;
-        k_ltree_level<F><<<grid_for(items), kBlock, 0, st>>>(refs, nslots, level, cnt_in, src, src_stride, dst,
-                                                              dst_stride, leaf_out, (const Ctx*)ctx, status);
+        const unsigned b = tune().level_block;
+        k_ltree_level<F><<<grid_for(items, b), b, 0, st>>>(refs, nslots, level, cnt_in, src, src_stride, dst,
+                                                            dst_stride, leaf_out, (const Ctx*)ctx, status);
     }
     static void tree_level(const TreeJob* jobs, uint32_t njobs, int h, int level, uint8_t* nodes, const void* ctx,
                            cudaStream_t st)
     {
         const uint64_t items = (uint64_t)njobs << (h - level - 1);
         if (!items) return;
-        k_tree_level<F><<<grid_for(items), kBlock, 0, st>>>(jobs, njobs, h, level, nodes, (const Ctx*)ctx);
+        const unsigned b = tune().level_block;
+        k_tree_level<F><<<grid_for(items, b), b, 0, st>>>(jobs, njobs, h, level, nodes, (const Ctx*)ctx);
     }
     static void verify_partition(const VerifyArgs& v, uint32_t blocks_max, uint32_t* sel_short, uint32_t* sel_long,
                                  uint32_t* n2, cudaStream_t st)
@@ -75,7 +80,8 @@ struct Launch {
     {
         const uint64_t items = (uint64_t)v.count * F::LEN;
         if (!items) return;
-        k_verify_chains<FT><<<grid_for(items), kBlock, 0, st>>>(v, layer, (const typename FT::Ctx*)ctx);
+        const unsigned b = tune().verify_chain_block;
+        k_verify_chains<FT><<<grid_for(items, b), b, 0, st>>>(v, layer, (const typename FT::Ctx*)ctx);
     }
     static void verify_ltree(const VerifyArgs& v, uint32_t layer, int cnt_in, uint32_t node_base,
                              const uint8_t* src, uint32_t src_stride, uint8_t* dst, uint32_t dst_stride,
@@ -83,8 +89,9 @@ struct Launch {
     {
         const uint64_t items = (uint64_t)v.count * ((cnt_in + 1) / 2);
         if (!items) return;
-        k_verify_ltree<F><<<grid_for(items), kBlock, 0, st>>>(v, layer, cnt_in, node_base, src, src_stride, dst,
-                                                              dst_stride);
+        const unsigned b = tune().level_block;
+        k_verify_ltree<F><<<grid_for(items, b), b, 0, st>>>(v, layer, cnt_in, node_base, src, src_stride, dst,
+                                                            dst_stride);
     }
     static void verify_root(const VerifyArgs& v, uint32_t layer, cudaStream_t st)
     {
@@ -100,7 +107,8 @@ struct Launch {
     {
         const uint64_t items = (uint64_t)g.count * g.d * F::LEN;
         if (!items) return;
-        k_sign_chains<FT><<<grid_for(items), kBlock, 0, st>>>(g, (const typename FT::Ctx*)ctx);
+        const unsigned b = tune().keygen_chain_block;
+        k_sign_chains<FT><<<grid_for(items, b), b, 0, st>>>(g, (const typename FT::Ctx*)ctx);
     }
     static void core_hash(const uint8_t* msgs, const uint64_t* off, const uint64_t* len, uint32_t count,
                           uint8_t* out, cudaStream_t st)
@@ -112,6 +120,7 @@ struct Launch {
     static FamilyOps table(const char* name, unsigned func)
     {
         FamilyOps o{};
+        s_func = func;
         o.name = name;
         o.func = func;
         o.n = (unsigned)F::N;

@@ -45,6 +45,17 @@ struct FamilyOps {
 // nullptr when (func, n) has no instantiation.
 const FamilyOps* family_ops(unsigned func, unsigned n);
 
+// Launch shapes of one hash family (set by the autotuner, tune.cu).  CTA
+// sizes are 32, 64 or 128 threads.
+struct Tuning {
+    uint32_t verify_chain_block = 128;  // k_verify_chains
+    uint32_t keygen_chain_block = 128;  // k_keygen_chains, k_sign_chains
+    uint32_t level_block = 128;         // L-tree and Merkle-level kernels
+    uint32_t split_min = 1024;          // verify batches this large run as two groups ...
+    uint32_t short_hmsg_blocks = 16;    // ... split at this many H_msg blocks
+};
+Tuning& tuning_for(unsigned func, unsigned n);
+
 extern const FamilyOps kOpsSha256N32;
 extern const FamilyOps kOpsSha256N24;
 extern const FamilyOps kOpsSha512N64;

@@ -117,6 +117,19 @@ lib.xmss_b200_verify_graph_create.argtypes = [C.c_uint32, C.c_int, C.c_uint32] +
 lib.xmss_b200_verify_graph_launch.argtypes = [C.c_void_p, C.c_void_p]
 lib.xmss_b200_verify_graph_destroy.argtypes = [C.c_void_p]
 lib.xmss_b200_verify_graph_destroy.restype = None
+class Tuning(C.Structure):
+    """xmss_b200_tuning (include/xmss_b200.h)."""
+
+    _fields_ = [(k, C.c_uint32) for k in ("verify_chain_block", "keygen_chain_block", "level_block", "split_min",
+                                          "short_hmsg_blocks")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+lib.xmss_b200_tuning_get.argtypes = [C.c_uint, C.c_uint, C.POINTER(Tuning)]
+lib.xmss_b200_tuning_set.argtypes = [C.c_uint, C.c_uint, C.POINTER(Tuning)]
+lib.xmss_b200_autotune.argtypes = [C.c_uint32, C.c_int, C.c_uint32, C.POINTER(Tuning), C.c_char_p, C.c_size_t]
 lib.xmss_b200_sign_batch.argtypes = [C.c_int, C.c_uint32, _u8p, _u8p, _u64p, _u64p, _u8p, _u64p,
                                      _u64p, _intp]
 lib.xmss_b200_core_hash_batch.argtypes = [C.c_uint, C.c_uint, C.c_uint32, _u8p, _u64p, _u64p, _u8p]
@@ -715,3 +728,62 @@ class VerifyGraph:
             self.close()
         except Exception:
             pass
+
+
+# -- launch-shape tuning ------------------------------------------------------
+
+FAMILIES = ((XMSS_SHA2, 24), (XMSS_SHA2, 32), (XMSS_SHA2, 64), (XMSS_SHAKE128, 32), (XMSS_SHAKE256, 24),
+            (XMSS_SHAKE256, 32), (XMSS_SHAKE256, 64))
+TUNING_PATH = os.path.join(HERE, "tuning.json")
+
+
+def tuning_get(func: int, n: int) -> dict:
+    t = Tuning()
+    if lib.xmss_b200_tuning_get(func, n, C.byref(t)):
+        raise ValueError(f"no family ({func}, {n})")
+    return t.as_dict()
+
+
+def tuning_set(func: int, n: int, shape: dict) -> None:
+    t = Tuning(**{k: int(shape[k]) for k, _ in Tuning._fields_})
+    if lib.xmss_b200_tuning_set(func, n, C.byref(t)):
+        raise ValueError(f"tuning_set({func}, {n}): {last_error()}")
+
+
+def autotune(oid: int, mt: bool, count: int = 4096):
+    """xmss_b200_autotune: returns (chosen shape, report of every trial)."""
+    import json
+
+    best = Tuning()
+    rep = C.create_string_buffer(1 << 16)
+    r = _check(lib.xmss_b200_autotune(oid, int(mt), count, C.byref(best), rep, len(rep)), "autotune")
+    if r:
+        raise ValueError(f"autotune returned {r}: {last_error()}")
+    return best.as_dict(), json.loads(rep.value.decode())
+
+
+def save_tuning(path: str = TUNING_PATH, notes: dict | None = None) -> None:
+    """Writes the current shape of every family as a JSON table."""
+    import json
+
+    table = {"families": [{"func": f, "n": n, **tuning_get(f, n)} for f, n in FAMILIES]}
+    if notes:
+        table["notes"] = notes
+    with open(path, "w") as fh:
+        json.dump(table, fh, indent=1)
+
+
+def load_tuning(path: str = TUNING_PATH) -> bool:
+    """Applies a table written by save_tuning; False when there is none."""
+    import json
+
+    if not os.path.exists(path):
+        return False
+    for e in json.load(open(path))["families"]:
+        tuning_set(e["func"], e["n"], e)
+    return True
+
+
+# the shapes measured on this GPU type, when a table sits next to the library
+if os.environ.get("XMSS_B200_TUNING", "1") != "0":
+    load_tuning(os.environ.get("XMSS_B200_TUNING_FILE", TUNING_PATH))

@@ -99,6 +99,33 @@ int xmss_b200_verify_graph_create(uint32_t oid, int mt, uint32_t count, const ui
 int xmss_b200_verify_graph_launch(xmss_b200_verify_graph *g, void *stream);
 void xmss_b200_verify_graph_destroy(xmss_b200_verify_graph *g);
 
+/* Launch shapes of one hash family (func, n): CTA sizes (32, 64 or 128
+ * threads) of the verify chain kernel, of the keygen / sign chain kernels
+ * and of the L-tree / Merkle-level kernels, and the split of large verify
+ * batches into a short- and a long-H_msg group on two streams (from
+ * split_min signatures on, at short_hmsg_blocks hash blocks).  Results do
+ * not depend on them.  Defaults: 128, 128, 128, 1024, 16.  Set them while no
+ * call of that family runs (they are read at each launch). */
+typedef struct {
+    uint32_t verify_chain_block;
+    uint32_t keygen_chain_block;
+    uint32_t level_block;
+    uint32_t split_min;
+    uint32_t short_hmsg_blocks;
+} xmss_b200_tuning;
+
+int xmss_b200_tuning_get(unsigned int func, unsigned int n, xmss_b200_tuning *out);
+int xmss_b200_tuning_set(unsigned int func, unsigned int n, const xmss_b200_tuning *t);
+
+/* Autotuner: times candidate shapes on a synthetic batch of this parameter
+ * set (16 seeded keys, `count` signatures of messages log-uniform in
+ * 32 B..4 KB, made by this library, and a 4,096-leaf keygen slice), one knob
+ * at a time, checks that every candidate accepts every signature, and
+ * leaves the fastest shape set for the family.  best gets it; report (if
+ * not NULL) a JSON text of every trial.  0 ok, -1 bad argument, -3 failure. */
+int xmss_b200_autotune(uint32_t oid, int mt, uint32_t count, xmss_b200_tuning *best, char *report,
+                       size_t report_cap);
+
 /* Batched xmss[mt]_sign (xmss.c:28-43, 78-93).  Request i signs
  * msgs[m_off[i] .. + mlen[i]) with sk i (sk: count x (4 + sk_bytes),
  * OID-prefixed, one OID), advancing that sk in place exactly as

@@ -74,3 +74,23 @@ def test_binding_argtypes_match_headers(xb):
             assert len(fn.argtypes) == nargs, (name, len(fn.argtypes), nargs)
             checked += 1
     assert checked >= 25
+
+
+def test_tuning_table_without_gpu(xb):
+    """Launch shapes are host state: readable and settable without a GPU,
+    validated (CTA sizes 32, 64, 128), one entry per hash family."""
+    for f, n in xb.FAMILIES:
+        t = xb.tuning_get(f, n)
+        assert t["verify_chain_block"] in (32, 64, 128) and t["split_min"] >= 1
+    old = xb.tuning_get(0, 32)
+    try:
+        xb.tuning_set(0, 32, dict(old, level_block=64))
+        assert xb.tuning_get(0, 32)["level_block"] == 64
+        assert xb.tuning_get(0, 24)["level_block"] == xb.tuning_get(0, 24)["level_block"]
+        for bad in (dict(old, verify_chain_block=256), dict(old, level_block=100), dict(old, split_min=0)):
+            with pytest.raises(ValueError):
+                xb.tuning_set(0, 32, bad)
+        with pytest.raises(ValueError):
+            xb.tuning_set(1, 64, old)  # no SHAKE128 n = 64 family
+    finally:
+        xb.tuning_set(0, 32, old)

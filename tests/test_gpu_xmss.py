@@ -400,3 +400,43 @@ def test_verify_graph_replays(xb, count):
         torch.cuda.synchronize()
         assert (d_st.cpu().numpy() == b[4]).all(), rep
     g.close()
+
+
+def test_results_do_not_depend_on_launch_shape(xb, golden):
+    """Every tunable shape (CTA sizes 32 / 64 / 128, split on or off at any
+    H_msg boundary) gives the same accept bitmap and the same keys; the
+    autotuner runs, checks its candidates and leaves a valid shape."""
+    rng = np.random.default_rng(97)
+    keys, count = 3, 1200
+    seeds = np.frombuffer(rng.bytes(keys * 96), np.uint8).reshape(keys, 96)
+    base = xb.tuning_get(0, 32)
+    pks, sks = xb.keypair_batch(1, False, seeds)
+    keyix = rng.integers(0, keys, count).astype(np.uint32)
+    rows = np.array(sks[keyix])
+    idx = rng.integers(0, 1023, count)
+    for i in range(count):
+        rows[i, 4:8] = np.frombuffer(int(idx[i]).to_bytes(4, "big"), np.uint8)
+    msgs = [rng.bytes(int(L)) for L in np.exp(rng.uniform(0, np.log(4000), count)).astype(int)]
+    _, sms = xb.sign_batch(False, rows.copy(), msgs)
+    sms = [bytearray(s) for s in sms]
+    for i in range(0, count, 6):
+        sms[i][int(rng.integers(0, len(sms[i])))] ^= 1
+    buf, off, ln = xb.pack([bytes(s) for s in sms], align=16)
+    want = xb.sign_open_batch(False, buf, off, ln, pks, keyix)
+    try:
+        for shape in (dict(base, verify_chain_block=32, level_block=32, keygen_chain_block=32),
+                      dict(base, verify_chain_block=64, level_block=128, keygen_chain_block=64, split_min=1,
+                           short_hmsg_blocks=8),
+                      dict(base, split_min=1 << 30)):
+            xb.tuning_set(0, 32, shape)
+            assert (xb.sign_open_batch(False, buf, off, ln, pks, keyix) == want).all(), shape
+            pk2, sk2 = xb.keypair_batch(1, False, seeds)
+            assert (pk2 == pks).all() and (sk2 == sks).all(), shape
+            _, sms2 = xb.sign_batch(False, rows.copy()[:20], msgs[:20])
+            r, _, sm0 = xb.xmss_sign(bytes(rows[0]), msgs[0])
+            assert sms2[0] == sm0
+        best, report = xb.autotune(1, False, 512)
+        assert best["verify_chain_block"] in (32, 64, 128) and len(report["trials"]) >= 10
+        assert xb.tuning_get(0, 32) == best
+    finally:
+        xb.tuning_set(0, 32, base)
