@@ -406,12 +406,13 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     return out
 
 
-def keygen_rate(xb, torch, dev, sh):
-    """Batched keygen of the survey's config 3: 8 XMSS-SHA2_16_256 keys and
-    1 XMSS-SHA2_20_256 key from seeded seeds, in one timed region."""
+def keygen_rate(xb, torch, dev, sh, sets=((0x02, 8), (0x03, 1))):
+    """Batched keygen of config 3: 8 XMSS-SHA2_16_256 keys and 1
+    XMSS-SHA2_20_256 key from seeded seeds, in one timed region (`sets`
+    other (oid, keys) pairs, e.g. one h=16 key for a profiler capture)."""
     rng = np.random.default_rng(SEED + 16)
     jobs = []
-    for oid, count in ((0x02, 8), (0x03, 1)):
+    for oid, count in sets:
         p = xb.parse_oid(oid)
         seeds = torch.from_numpy(np.frombuffer(rng.bytes(count * 3 * p.n), np.uint8).copy()).to(dev)
         d_pk = torch.empty(count * 2 * p.n, dtype=torch.uint8, device=dev)
@@ -433,9 +434,27 @@ def keygen_rate(xb, torch, dev, sh):
     leaves = sum(count << p.full_height for _, count, p, *_ in jobs)
     leaf_compr = 67 * 2 + 67 * 15 * 4 + 66 * 6  # PRF_keygen, 15 F per chain, L-tree
     comp = sum(count * ((leaf_compr << p.full_height) + 6 * ((1 << p.full_height) - 1)) for _, count, p, *_ in jobs)
-    return {"metric": "keygen leaves/s: 8 x XMSS-SHA2_16_256 + 1 x XMSS-SHA2_20_256 (1,572,864 leaves)",
+    what = " + ".join(f"{count} x XMSS-SHA2_{p.full_height}_256" for _, count, p, *_ in jobs)
+    return {"metric": f"keygen leaves/s: {what} ({leaves:,} leaves)",
             "value": leaves / (ms / 1e3), "unit": "leaves/s", "ms": ms, "gcompr_s": comp / (ms / 1e3) / 1e9,
             "compressions": comp}
+
+
+def run_keygen(args):
+    """Config 3 alone (--keygen-small: one XMSS-SHA2_16_256 key, the size
+    the profiler captures)."""
+    import torch
+
+    import xmss_b200 as xb
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    xb.init(0)
+    sh = torch.cuda.current_stream(dev).cuda_stream
+    sets = ((0x02, 1),) if args.keygen_small else ((0x02, 8), (0x03, 1))
+    out = keygen_rate(xb, torch, dev, sh, sets)
+    out["workload"] = "keygen"
+    return out
 
 
 def read_traffic():
@@ -624,8 +643,23 @@ def run_mix(args):
     import xmss_b200 as xb
 
     xb.init(0)
+    dev = torch.device("cuda", 0)
+    sh = torch.cuda.current_stream(dev).cuda_stream
+    # compression-rate probes of the three cores (same code as the kernels)
+    probe_blocks = 148 * 16 * 4
+    sink = torch.zeros(probe_blocks * 128, dtype=torch.int32, device=dev)
+    probe = {}
+    for kind, iters in ((10, 1000), (11, 1000), (2, 200), (1, 200)):
+        xb.rate_probe(kind, probe_blocks, 20, sink.data_ptr(), sh)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        xb.rate_probe(kind, probe_blocks, iters, sink.data_ptr(), sh)
+        e1.record()
+        torch.cuda.synchronize()
+        probe[kind] = probe_blocks * 128 * iters / (e0.elapsed_time(e1) / 1e3) / 1e9
     rng = np.random.default_rng(SEED + 4)
-    out = {"workload": "mix", "sets": []}
+    out = {"workload": "mix", "sets": [],
+           "probe_g_per_s": {"sha256": max(probe[10], probe[11]), "sha512": probe[2], "keccak_f1600": probe[1]}}
     for name, oid, mt in MIX_SETS:
         p = xb.parse_oid(oid, mt)
         count = 2048
@@ -658,7 +692,20 @@ def run_mix(args):
         st = xb.sign_open_batch(mt, buf, off, ln, pks, kix)
         t_ver = time.perf_counter() - t0
         w = xb.last_verify_work()
+        # chain kernels of one more (profiled, single-sequence) verify against
+        # the probe of their core: F = 4 SHA-256 / 4 SHA-512 compressions or
+        # 3 Keccak-f permutations with per-key midstates
+        xb.profile(True)
+        xb.sign_open_batch(mt, buf, off, ln, pks, kix)
+        chains_ms = xb.phase_ms()["chains"]
+        xb.profile(False)
+        core = "keccak_f1600" if p.func != 0 else ("sha512" if p.n == 64 else "sha256")
+        per_f = 3 if core == "keccak_f1600" else 4
+        achieved = w.f_calls * per_f / (chains_ms / 1e3) / 1e9
+        roof = {"core": core, "achieved_g_per_s": achieved, "peak_g_per_s": out["probe_g_per_s"][core],
+                "frac": achieved / out["probe_g_per_s"][core], "chains_ms": chains_ms}
         out["sets"].append({"set": name, "keys": nkeys, "signs": count, "signs_per_s": count / t_sign,
+                            "chain_roofline": roof,
                             "verifies_per_s": count / t_ver, "sign_s": t_sign, "verify_s": t_ver,
                             "mean_mlen": float(mlen.mean()), "all_signed": bool((ret == 0).all()),
                             "all_verified": bool((st == 0).all()),
@@ -897,7 +944,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["verify", "mix", "plain", "serve"], default="verify",
+    ap.add_argument("--workload", choices=["verify", "mix", "plain", "serve", "keygen"], default="verify",
                     help="verify: the headline line; mix / plain / serve: the XMSS^MT + wide-hash, per-call "
                          "and serving configs")
     ap.add_argument("--serve-rates", default="10000,30000,100000,300000,1000000",
@@ -907,6 +954,7 @@ def main():
     ap.add_argument("--serve-batch", type=int, default=4096)
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--serve-plain-n", type=int, default=150, help="requests of the per-call comparison")
+    ap.add_argument("--keygen-small", action="store_true", help="keygen workload: one h=16 key (profiling)")
     ap.add_argument("--skip-keygen", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=2.5)
@@ -934,6 +982,8 @@ def main():
         out = run_plain(args)
     elif args.workload == "serve":
         out = run_serve(args)
+    elif args.workload == "keygen":
+        out = run_keygen(args)
     else:
         out = run_ours(args, rank, world, local_rank)
     if out is not None:

@@ -50,7 +50,31 @@ __global__ void __launch_bounds__(128) k_keccak_rate(uint32_t iters, uint32_t se
     if ((uint32_t)x == 0x9E3779B9u) sink[t] = (uint32_t)x;
 }
 
+__global__ void __launch_bounds__(128) k_sha512_rate(uint32_t iters, uint32_t seed, uint32_t* __restrict__ sink)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t st[8];
+    sha512_iv(st);
+    st[0] ^= t;
+    st[1] ^= seed;
+#pragma unroll 1
+    for (uint32_t i = 0; i < iters; i++) {
+        uint64_t w[16];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            w[j] = st[j];
+            w[8 + j] = st[j] ^ i;
+        }
+        sha512_compress(st, w);
+    }
+    uint64_t x = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) x ^= st[j];
+    if ((uint32_t)x == 0x9E3779B9u) sink[t] = (uint32_t)x;
+}
+
 // kind 0: SHA-256 as the XMSS kernels compile it; 1: Keccak-f[1600];
+// 2: SHA-512 compressions;
 // 10 + m: SHA-256 with pipe mix m (for comparing the variants);
 // 20 + m: the same with one warp per block (latency of a lone thread).
 void launch_rate(int kind, uint32_t blocks, uint32_t iters, uint32_t* sink, cudaStream_t st)
@@ -62,6 +86,7 @@ void launch_rate(int kind, uint32_t blocks, uint32_t iters, uint32_t* sink, cuda
         case 23: k_sha256_rate<3><<<blocks, 32, 0, st>>>(iters, 0x1234567u, sink); break;
         case 0: k_sha256_rate<XB_SHA256_MIX><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
         case 1: k_keccak_rate<<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 2: k_sha512_rate<<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
         case 10: k_sha256_rate<0><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
         case 11: k_sha256_rate<1><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
         case 12: k_sha256_rate<2><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;

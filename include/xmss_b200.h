@@ -349,8 +349,9 @@ int xmss_b200_sk_from_bds(int mt, const uint8_t *bds_sk, uint8_t *sk);
 int xmss_b200_sk_to_bds(int mt, const uint8_t *sk, uint8_t *bds_sk);
 
 /* Compression-rate probe (the roofline denominator): `blocks` x 128 threads
- * each run `iters` dependent SHA-256 compressions (kind 0) or Keccak-f[1600]
- * permutations (kind 1) in registers, on `stream`.  d_sink: blocks x 128
+ * each run `iters` dependent SHA-256 compressions (kind 0), Keccak-f[1600]
+ * permutations (kind 1) or SHA-512 compressions (kind 2) in registers, on
+ * `stream`.  d_sink: blocks x 128
  * u32 of device memory (written almost never). */
 int xmss_b200_rate_probe(int kind, uint32_t blocks, uint32_t iters, uint32_t *d_sink, void *stream);
 
