@@ -694,6 +694,77 @@ struct Sha512N64 : FamBase<64, 64, true> {
         sha512_compress(st, w);
     }
 
+    // The WOTS chain (wots.c:38-53) as one loop over compression sub-steps -
+    // PRF key, toByte(0, 64) || key, PRF mask, (x ^ mask) || padding per F
+    // call, PRF_keygen first for keygen - so a chain kernel holds a single
+    // SHA-512 compression body.
+    static constexpr bool kHasChain = true;
+
+    __device__ static void chain(uint32_t (&x)[16], const Ctx& c, const uint32_t (&a)[8], uint32_t start,
+                                 uint32_t steps, bool keygen)
+    {
+        uint64_t tmp[8], mask[8];  // key, then the state after toByte(0) || key; the mask
+        const uint32_t pre = keygen ? 1 : 0;
+        const uint32_t total = pre + 4 * steps;
+#pragma unroll 1
+        for (uint32_t j = 0; j < total; j++) {
+            uint64_t st[8], w[16];
+            const uint32_t jj = j - pre;
+            const uint32_t phase = (j < pre) ? 4 : (jj & 3);
+            const uint32_t hash = start + (jj >> 2);
+            if (phase == 0 || phase == 2) {  // PRF(PUB_SEED, ADRS), key_and_mask 0 (key) or 1 (mask)
+#pragma unroll
+                for (int i = 0; i < 3; i++) w[i] = join64(a[2 * i], a[2 * i + 1]);
+                w[3] = join64(hash, phase >> 1);
+                w[4] = 0x8000000000000000ull;
+#pragma unroll
+                for (int i = 5; i < 15; i++) w[i] = 0;
+                w[15] = 1280;  // (64 + 64 + 32) * 8
+#pragma unroll
+                for (int i = 0; i < 8; i++) st[i] = c.prf_mid[i];
+            } else if (phase == 1) {  // toByte(0, 64) || key from the IV
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    w[i] = 0;
+                    w[8 + i] = tmp[i];
+                }
+                sha512_iv(st);
+            } else if (phase == 3) {  // (x ^ mask) || padding of 192 bytes
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    w[i] = join64(x[2 * i], x[2 * i + 1]) ^ mask[i];
+                    st[i] = tmp[i];
+                }
+                w[8] = 0x8000000000000000ull;
+#pragma unroll
+                for (int i = 9; i < 15; i++) w[i] = 0;
+                w[15] = 1536;  // 192 * 8
+            } else {  // PRF_keygen: PUB_SEED || ADRS from the SK_SEED midstate
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    w[i] = join64(c.pub[2 * i], c.pub[2 * i + 1]);
+                    st[i] = c.kg_mid[i];
+                }
+#pragma unroll
+                for (int i = 0; i < 4; i++) w[8 + i] = join64(a[2 * i], a[2 * i + 1]);
+                w[12] = 0x8000000000000000ull;
+                w[13] = 0;
+                w[14] = 0;
+                w[15] = 1792;  // (64 + 64 + 64 + 32) * 8
+            }
+            sha512_compress(st, w);
+            if (phase <= 1) {
+#pragma unroll
+                for (int i = 0; i < 8; i++) tmp[i] = st[i];
+            } else if (phase == 2) {
+#pragma unroll
+                for (int i = 0; i < 8; i++) mask[i] = st[i];
+            } else {
+                out16(x, st);
+            }
+        }
+    }
+
     __device__ static void thash_f(uint32_t (&x)[16], const Ctx& c, uint32_t (&a)[8])
     {
         uint64_t t[8], st[8], w[16];

@@ -165,9 +165,9 @@ __device__ __forceinline__ void sha256_words(uint32_t (&out)[8], const uint32_t 
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint64_t ror64(uint64_t x, int n) { return (x >> n) | (x << (64 - n)); }
 
-__device__ __forceinline__ void sha512_compress(uint64_t (&st)[8], uint64_t (&w)[16])
-{
-    const uint64_t K[80] = {
+// Round constants in constant memory: the rounds after the first 16 run as
+// a loop over 16-round blocks (see sha512_compress).
+static __constant__ uint64_t kSha512K[80] = {
         0x428a2f98d728ae22ull, 0x7137449123ef65cdull, 0xb5c0fbcfec4d3b2full, 0xe9b5dba58189dbbcull,
         0x3956c25bf348b538ull, 0x59f111f1b605d019ull, 0x923f82a4af194f9bull, 0xab1c5ed5da6d8118ull,
         0xd807aa98a3030242ull, 0x12835b0145706fbeull, 0x243185be4ee4b28cull, 0x550c7dc3d5ffb4e2ull,
@@ -188,26 +188,49 @@ __device__ __forceinline__ void sha512_compress(uint64_t (&st)[8], uint64_t (&w)
         0x06f067aa72176fbaull, 0x0a637dc5a2c898a6ull, 0x113f9804bef90daeull, 0x1b710b35131c471bull,
         0x28db77f523047d84ull, 0x32caab7b40c72493ull, 0x3c9ebe0a15c9bebcull, 0x431d67c49c100d4cull,
         0x4cc5d4becb3e42b6ull, 0x597f299cfc657e2aull, 0x5fcb6fab3ad6faecull, 0x6c44198c4a475817ull};
-    uint64_t a = st[0], b = st[1], c = st[2], d = st[3];
-    uint64_t e = st[4], f = st[5], g = st[6], h = st[7];
+
+// One round on the state v[8] whose roles rotate: at round j, a is
+// v[(8 - j) & 7] ... h is v[(15 - j) & 7]; j is a compile-time constant once
+// the caller's loop is unrolled, so v stays in registers.
+__device__ __forceinline__ void sha512_round(uint64_t (&v)[8], int j, uint64_t k, uint64_t wj)
+{
+    const uint64_t a = v[(8 - j) & 7], b = v[(9 - j) & 7], c = v[(10 - j) & 7];
+    const uint64_t e = v[(12 - j) & 7], f = v[(13 - j) & 7], g = v[(14 - j) & 7];
+    const uint64_t S1 = ror64(e, 14) ^ ror64(e, 18) ^ ror64(e, 41);
+    const uint64_t ch = g ^ (e & (f ^ g));
+    const uint64_t t1 = v[(15 - j) & 7] + S1 + ch + k + wj;
+    const uint64_t S0 = ror64(a, 28) ^ ror64(a, 34) ^ ror64(a, 39);
+    const uint64_t mj = (a & b) | (c & (a | b));
+    v[(11 - j) & 7] += t1;           // d + t1 is the next round's e
+    v[(15 - j) & 7] = t1 + S0 + mj;  // the slot of h holds the next round's a
+}
+
+// FIPS 180-4 6.4.2.  The first 16 rounds take the message words as they
+// are; rounds 16..79 run as four passes of one unrolled 16-round block that
+// extends the schedule in place (16 is a multiple of 8, so the state roles
+// line up from pass to pass).  The rolled form keeps a kernel's SHA-512 code
+// small: fully unrolled, the four compressions of an F call did not stay in
+// the instruction cache (instruction fetch was the top stall).
+__device__ __forceinline__ void sha512_compress(uint64_t (&st)[8], uint64_t (&w)[16])
+{
+    uint64_t v[8];
 #pragma unroll
-    for (int t = 0; t < 80; t++) {
-        if (t >= 16) {
-            const uint64_t x15 = w[(t - 15) & 15], x2 = w[(t - 2) & 15];
+    for (int i = 0; i < 8; i++) v[i] = st[i];
+#pragma unroll
+    for (int j = 0; j < 16; j++) sha512_round(v, j, kSha512K[j], w[j]);
+#pragma unroll 1
+    for (int r = 16; r < 80; r += 16) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const uint64_t x15 = w[(j + 1) & 15], x2 = w[(j + 14) & 15];
             const uint64_t s0 = ror64(x15, 1) ^ ror64(x15, 8) ^ (x15 >> 7);
             const uint64_t s1 = ror64(x2, 19) ^ ror64(x2, 61) ^ (x2 >> 6);
-            w[t & 15] += s0 + w[(t - 7) & 15] + s1;
+            w[j] += s0 + w[(j + 9) & 15] + s1;
+            sha512_round(v, j, kSha512K[r + j], w[j]);
         }
-        const uint64_t S1 = ror64(e, 14) ^ ror64(e, 18) ^ ror64(e, 41);
-        const uint64_t ch = g ^ (e & (f ^ g));
-        const uint64_t t1 = h + S1 + ch + K[t] + w[t & 15];
-        const uint64_t S0 = ror64(a, 28) ^ ror64(a, 34) ^ ror64(a, 39);
-        const uint64_t mj = (a & b) | (c & (a | b));
-        h = g; g = f; f = e; e = d + t1;
-        d = c; c = b; b = a; a = t1 + S0 + mj;
     }
-    st[0] += a; st[1] += b; st[2] += c; st[3] += d;
-    st[4] += e; st[5] += f; st[6] += g; st[7] += h;
+#pragma unroll
+    for (int i = 0; i < 8; i++) st[i] += v[i];
 }
 
 __device__ __forceinline__ void sha512_iv(uint64_t (&st)[8])
