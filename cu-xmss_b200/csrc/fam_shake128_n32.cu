@@ -3,5 +3,5 @@
 #include "family_ops.cuh"
 
 namespace xb {
-const FamilyOps kOpsShake128N32 = Launch<Shake128N32>::table("Shake128N32", XMSS_SHAKE128);
+const FamilyOps kOpsShake128N32 = Launch<Shake128N32, Shake128N32Chain>::table("Shake128N32", XMSS_SHAKE128);
 }  // namespace xb

@@ -3,5 +3,5 @@
 #include "family_ops.cuh"
 
 namespace xb {
-const FamilyOps kOpsShake256N24 = Launch<Shake256N24>::table("Shake256N24", XMSS_SHAKE256);
+const FamilyOps kOpsShake256N24 = Launch<Shake256N24, Shake256N24Chain>::table("Shake256N24", XMSS_SHAKE256);
 }  // namespace xb

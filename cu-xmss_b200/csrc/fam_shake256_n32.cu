@@ -3,5 +3,5 @@
 #include "family_ops.cuh"
 
 namespace xb {
-const FamilyOps kOpsShake256N32 = Launch<Shake256N32>::table("Shake256N32", XMSS_SHAKE256);
+const FamilyOps kOpsShake256N32 = Launch<Shake256N32, Shake256N32Chain>::table("Shake256N32", XMSS_SHAKE256);
 }  // namespace xb

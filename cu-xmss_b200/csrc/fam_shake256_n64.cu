@@ -3,5 +3,5 @@
 #include "family_ops.cuh"
 
 namespace xb {
-const FamilyOps kOpsShake256N64 = Launch<Shake256N64>::table("Shake256N64", XMSS_SHAKE256);
+const FamilyOps kOpsShake256N64 = Launch<Shake256N64, Shake256N64Chain>::table("Shake256N64", XMSS_SHAKE256);
 }  // namespace xb

@@ -297,13 +297,14 @@ struct CoreSha256 {
     }
 };
 
-template <int RATEW>
+// ROLL < 24: the permutation runs ROLL rounds per loop pass (chain kernels).
+template <int RATEW, int ROLL = 24>
 struct CoreShake {
     static constexpr bool BE = false;
     template <int MW, int OW>
     __device__ __forceinline__ static void digest(uint32_t (&out)[OW], const uint32_t (&m)[MW])
     {
-        shake_words<RATEW, MW, OW>(out, m);
+        shake_words<RATEW, MW, OW, ROLL>(out, m);
     }
 };
 
@@ -312,6 +313,16 @@ using Shake128N32 = GenericFam<CoreShake<42>, 32, 32>;
 using Shake256N24 = GenericFam<CoreShake<34>, 24, 4>;
 using Shake256N32 = GenericFam<CoreShake<34>, 32, 32>;
 using Shake256N64 = GenericFam<CoreShake<34>, 64, 64>;
+
+// The chain kernels' form of the SHAKE families (same key context): the
+// permutation partly rolled, so that their F calls fit the instruction cache.
+#ifndef XB_KECCAK_CHAIN_ROLL
+#define XB_KECCAK_CHAIN_ROLL 4
+#endif
+using Shake128N32Chain = GenericFam<CoreShake<42, XB_KECCAK_CHAIN_ROLL>, 32, 32>;
+using Shake256N24Chain = GenericFam<CoreShake<34, XB_KECCAK_CHAIN_ROLL>, 24, 4>;
+using Shake256N32Chain = GenericFam<CoreShake<34, XB_KECCAK_CHAIN_ROLL>, 32, 32>;
+using Shake256N64Chain = GenericFam<CoreShake<34, XB_KECCAK_CHAIN_ROLL>, 64, 64>;
 
 // ---------------------------------------------------------------------------
 // SHA-256, n = 32, padding_len = 32: midstate form.

@@ -337,9 +337,49 @@ __device__ __forceinline__ void keccak_f1600(uint64_t (&A)[25])
     }
 }
 
+// Round constants for the partly rolled permutation below.
+static __constant__ uint64_t kKeccakRC[24] = {
+    0x0000000000000001ull, 0x0000000000008082ull, 0x800000000000808aull, 0x8000000080008000ull,
+    0x000000000000808bull, 0x0000000080000001ull, 0x8000000080008081ull, 0x8000000000008009ull,
+    0x000000000000008aull, 0x0000000000000088ull, 0x0000000080008009ull, 0x000000008000000aull,
+    0x000000008000808bull, 0x800000000000008bull, 0x8000000000008089ull, 0x8000000000008003ull,
+    0x8000000000008002ull, 0x8000000000000080ull, 0x000000000000800aull, 0x800000008000000aull,
+    0x8000000080008081ull, 0x8000000000008080ull, 0x0000000080000001ull, 0x8000000080008008ull};
+
+// Keccak-f[1600] with U rounds per loop pass (U divides 24): the form for
+// the throughput-bound chain kernels, whose fully unrolled F call (three
+// permutations) does not stay in the instruction cache.  The serial H_msg
+// keeps keccak_f1600: rolling measured 1.5x its latency.
+template <int U>
+__device__ __forceinline__ void keccak_f1600_u(uint64_t (&A)[25])
+{
+    static_assert(24 % U == 0, "U must divide 24");
+#pragma unroll 1
+    for (int r = 0; r < 24; r += U) {
+#pragma unroll
+        for (int q = 0; q < U; q++) {
+            uint64_t C[5], D[5], B[25];
+#pragma unroll
+            for (int x = 0; x < 5; x++) C[x] = A[x] ^ A[x + 5] ^ A[x + 10] ^ A[x + 15] ^ A[x + 20];
+#pragma unroll
+            for (int x = 0; x < 5; x++) D[x] = C[(x + 4) % 5] ^ rol64c<1>(C[(x + 1) % 5]);
+            keccak_rho_pi<0>(B, A, D);
+#pragma unroll
+            for (int y = 0; y < 5; y++) {
+#pragma unroll
+                for (int x = 0; x < 5; x++) {
+                    A[x + 5 * y] = B[x + 5 * y] ^ (~B[(x + 1) % 5 + 5 * y] & B[(x + 2) % 5 + 5 * y]);
+                }
+            }
+            A[0] ^= kKeccakRC[r + q];
+        }
+    }
+}
+
 // SHAKE with rate RATEW 32-bit words (42 = SHAKE128, 34 = SHAKE256) over a
 // message of MW little-endian words; writes the first OUTW output words.
-template <int RATEW, int MW, int OUTW>
+// U < 24: the permutation runs U rounds per loop pass (keccak_f1600_u).
+template <int RATEW, int MW, int OUTW, int U = 24>
 __device__ __forceinline__ void shake_words(uint32_t (&out)[OUTW], const uint32_t (&m)[MW])
 {
     static_assert(OUTW <= RATEW, "output fits in one squeeze block");
@@ -360,7 +400,11 @@ __device__ __forceinline__ void shake_words(uint32_t (&out)[OUTW], const uint32_
             if (b == NB - 1 && 2 * i + 1 == RATEW - 1) hi ^= 0x80000000u;
             A[i] ^= ((uint64_t)hi << 32) | lo;
         }
-        keccak_f1600(A);
+        if constexpr (U < 24) {
+            keccak_f1600_u<U>(A);
+        } else {
+            keccak_f1600(A);
+        }
     }
 #pragma unroll
     for (int i = 0; i < OUTW; i++) out[i] = (i & 1) ? (uint32_t)(A[i / 2] >> 32) : (uint32_t)A[i / 2];

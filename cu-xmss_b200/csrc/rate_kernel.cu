@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(128) k_keccak_rate(uint32_t iters, uint32_t se
 #pragma unroll 1
     for (uint32_t i = 0; i < iters; i++) {
         A[0] ^= i;
-        keccak_f1600(A);
+        keccak_f1600_u<4>(A);  // the form the chain kernels run (4 rounds per loop pass)
     }
     uint64_t x = 0;
 #pragma unroll
