@@ -320,7 +320,7 @@ void Engine::keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count,
 // One launch sequence of verify (prep, then per layer: bucket, chains, L-tree,
 // root) over the signatures v selects, on stream st.
 void Engine::verify_sequence(const FamilyOps* ops, const xmss_params& p, const VerifyArgs& v, const void* ctx,
-                             cudaStream_t st, bool on)
+                             cudaStream_t st, bool on, bool fused_ltree)
 {
     const uint32_t len = ops->len;
     mark(kPrep, true, st, on);
@@ -332,16 +332,20 @@ void Engine::verify_sequence(const FamilyOps* ops, const xmss_params& p, const V
         ops->verify_chains(v, layer, ctx, st);
         mark(kChains, false, st, on);
         mark(kLtree, true, st, on);
-        int cnt = (int)len;
-        uint32_t node_base = 0;
-        uint8_t *src = v.wpk, *dst = v.wpk2;
-        uint32_t sstr = len, dstr = (len + 1) / 2;
-        while (cnt > 1) {
-            ops->verify_ltree(v, layer, cnt, node_base, src, sstr, dst, dstr, st);
-            node_base += cnt / 2;
-            cnt = (cnt + 1) / 2;
-            std::swap(src, dst);
-            std::swap(sstr, dstr);
+        if (fused_ltree) {
+            ops->verify_ltree_warp(v, layer, st);
+        } else {
+            int cnt = (int)len;
+            uint32_t node_base = 0;
+            uint8_t *src = v.wpk, *dst = v.wpk2;
+            uint32_t sstr = len, dstr = (len + 1) / 2;
+            while (cnt > 1) {
+                ops->verify_ltree(v, layer, cnt, node_base, src, sstr, dst, dstr, st);
+                node_base += cnt / 2;
+                cnt = (cnt + 1) / 2;
+                std::swap(src, dst);
+                std::swap(sstr, dstr);
+            }
         }
         mark(kLtree, false, st, on);
         mark(kRoot, true, st, on);
@@ -399,7 +403,7 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
     SplitStreams* ss = own ? &split_ : w.split;
     const Tuning& tn = tuning_for(ops->func, ops->n);
     if (!allow_split || count < tn.split_min || profiling || !ss) {
-        verify_sequence(ops, p, v, ctx, st, own);
+        verify_sequence(ops, p, v, ctx, st, own, count < kFusedLtreeBelow);
         return;
     }
     uint32_t* n2 = hist + 2 * 32 * p.d;

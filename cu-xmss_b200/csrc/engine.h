@@ -183,8 +183,15 @@ class Engine {
 
     // Verify launch sequence over the signatures v selects (all when
     // v.sel is null), on one stream.
+    // fused_ltree: the whole L-tree in one warp-per-signature launch (for
+    // groups whose L-tree runs with the GPU otherwise idle) instead of one
+    // launch per level.
     void verify_sequence(const FamilyOps* ops, const xmss_params& p, const VerifyArgs& v, const void* ctx,
-                         cudaStream_t st, bool marks = true);
+                         cudaStream_t st, bool marks = true, bool fused_ltree = false);
+    // Single-sequence batches below this size are latency-bound: fused
+    // L-tree (measured: it lowers serving latency at light load; for larger
+    // batches, and for the tail group of a split batch, it cost throughput).
+    static constexpr uint32_t kFusedLtreeBelow = 256;
     // Batches of at least Tuning::split_min signatures are verified as two
     // groups split at Tuning::short_hmsg_blocks hash blocks of H_msg.
 

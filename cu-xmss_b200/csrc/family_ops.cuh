@@ -93,6 +93,11 @@ struct Launch {
         k_verify_ltree<F><<<grid_for(items, b), b, 0, st>>>(v, layer, cnt_in, node_base, src, src_stride, dst,
                                                             dst_stride);
     }
+    static void verify_ltree_warp(const VerifyArgs& v, uint32_t layer, cudaStream_t st)
+    {
+        if (!v.count) return;
+        k_verify_ltree_warp<F><<<(v.count + 1) / 2, 64, 0, st>>>(v, layer);
+    }
     static void verify_root(const VerifyArgs& v, uint32_t layer, cudaStream_t st)
     {
         if (!v.count) return;
@@ -137,6 +142,7 @@ struct Launch {
         o.verify_chains = verify_chains;
         o.verify_ltree = verify_ltree;
         o.verify_root = verify_root;
+        o.verify_ltree_warp = verify_ltree_warp;
         o.sign_prep = sign_prep;
         o.sign_chains = sign_chains;
         o.core_hash = core_hash;

@@ -36,6 +36,7 @@ struct FamilyOps {
     void (*verify_ltree)(const VerifyArgs& v, uint32_t layer, int cnt_in, uint32_t node_base, const uint8_t* src,
                          uint32_t src_stride, uint8_t* dst, uint32_t dst_stride, cudaStream_t st);
     void (*verify_root)(const VerifyArgs& v, uint32_t layer, cudaStream_t st);
+    void (*verify_ltree_warp)(const VerifyArgs& v, uint32_t layer, cudaStream_t st);  // whole L-tree, warp / sig
     void (*sign_prep)(const SignArgs& g, const void* ctx, cudaStream_t st);
     void (*sign_chains)(const SignArgs& g, const void* ctx, cudaStream_t st);
     void (*core_hash)(const uint8_t* msgs, const uint64_t* off, const uint64_t* len, uint32_t count, uint8_t* out,

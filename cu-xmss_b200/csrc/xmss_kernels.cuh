@@ -505,6 +505,59 @@ __global__ void __launch_bounds__(128) k_verify_ltree(VerifyArgs v, uint32_t lay
     }
 }
 
+// The whole L-tree of one layer (xmss_commons.c:16-49) for a signature per
+// warp: its LEN WOTS public-key values go to shared memory, the lanes hash
+// the pairs of a level (h_fin with the precomputed h_pre), the odd node is
+// carried up, and the level's nodes stay in shared memory for the next; the
+// last level writes the leaf.  Same nodes, order and outputs as LEN - 1
+// launches of k_verify_ltree, in one launch: for latency-bound batches (a
+// warp instruction costs one issue slot however few lanes are active, so
+// where many warps compete for the ALU the per-level kernels are cheaper).
+template <class F>
+__global__ void __launch_bounds__(64) k_verify_ltree_warp(VerifyArgs v, uint32_t layer)
+{
+    using HPre = typename F::HPre;
+    constexpr int L0 = F::LEN, L1 = (F::LEN + 1) / 2;
+    __shared__ __align__(16) uint8_t sh[2][(L0 + L1) * F::N];
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    if (w >= sel_count(v)) return;
+    const uint32_t s = sel_sig(v, w);
+    if (v.status[s] != 0) return;
+    uint8_t* a = sh[threadIdx.x >> 5];
+    uint8_t* b = a + L0 * F::N;
+    // level 0 from the chain outputs (N is a multiple of 8)
+    const uint2* g = (const uint2*)(v.wpk + (uint64_t)s * L0 * F::N);
+    for (int i = lane; i < L0 * F::N / 8; i += 32) ((uint2*)a)[i] = g[i];
+    __syncwarp();
+    const uint32_t nh = F::LEN - 1 + v.tree_height;
+    const HPre* hp = (const HPre*)v.hpre + ((uint64_t)s * v.d + layer) * nh;
+    int cnt = L0;
+    uint32_t base = 0;
+    while (cnt > 1) {
+        const int pairs = (cnt + 1) >> 1;
+        for (int p = lane; p < pairs; p += 32) {
+            uint32_t l[F::NW], o[F::NW];
+            F::load(l, a + (uint64_t)(2 * p) * F::N);
+            if (2 * p + 1 < cnt) {
+                uint32_t r[F::NW];
+                F::load(r, a + (uint64_t)(2 * p + 1) * F::N);
+                F::h_fin(o, hp[base + p], l, r);
+            } else {
+#pragma unroll
+                for (int i = 0; i < F::NW; i++) o[i] = l[i];
+            }
+            F::store(cnt == 2 ? v.leaf + (uint64_t)s * F::N : b + (uint64_t)p * F::N, o);
+        }
+        __syncwarp();
+        base += cnt >> 1;
+        cnt = pairs;
+        uint8_t* t = a;
+        a = b;
+        b = t;
+    }
+}
+
 // compute_root (xmss_commons.c:54-96) for one layer with precomputed h_pre;
 // then either the next layer's chain lengths or the comparison with the
 // public root (xmss_commons.c:204-209).
