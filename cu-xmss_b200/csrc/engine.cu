@@ -54,8 +54,18 @@ void SplitStreams::create()
     // Equal priorities: giving the latency-bound phases (or one group) a
     // higher stream priority measured 7-14 % slower per batch.
     XB_CUDA(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
+    XB_CUDA(cudaStreamCreateWithFlags(&pre, cudaStreamNonBlocking));
     XB_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
     XB_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    XB_CUDA(cudaEventCreateWithFlags(&pre_done, cudaEventDisableTiming));
+}
+
+void SplitStreams::destroy()
+{
+    for (cudaStream_t* s : {&aux, &pre})
+        if (*s) cudaStreamDestroy(*s), *s = nullptr;
+    for (cudaEvent_t* e : {&fork, &join, &pre_done})
+        if (*e) cudaEventDestroy(*e), *e = nullptr;
 }
 
 void Workspace::order_on(cudaStream_t st)
@@ -318,19 +328,25 @@ void Engine::keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count,
 }
 
 // One launch sequence of verify (prep, then per layer: bucket, chains, L-tree,
-// root) over the signatures v selects, on stream st.
+// root) over the signatures v selects, on stream st.  With hpre_ready the
+// caller has launched the prep's parts itself: the H_msg part ahead on st,
+// the h_pre part elsewhere, ending at that event, which the first L-tree
+// waits for.
 void Engine::verify_sequence(const FamilyOps* ops, const xmss_params& p, const VerifyArgs& v, const void* ctx,
-                             cudaStream_t st, bool on, bool fused_ltree)
+                             cudaStream_t st, bool on, bool fused_ltree, cudaEvent_t hpre_ready)
 {
     const uint32_t len = ops->len;
-    mark(kPrep, true, st, on);
-    ops->verify_prep(v, ctx, st);
-    mark(kPrep, false, st, on);
+    if (!hpre_ready) {
+        mark(kPrep, true, st, on);
+        ops->verify_prep(v, ctx, st);
+        mark(kPrep, false, st, on);
+    }
     for (uint32_t layer = 0; layer < p.d; layer++) {
         mark(kChains, true, st, on);
         ops->verify_scatter(v, layer, st);
         ops->verify_chains(v, layer, ctx, st);
         mark(kChains, false, st, on);
+        if (layer == 0 && hpre_ready) XB_CUDA(cudaStreamWaitEvent(st, hpre_ready, 0));
         mark(kLtree, true, st, on);
         if (fused_ltree) {
             ops->verify_ltree_warp(v, layer, st);
@@ -419,8 +435,22 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
     b.list = w.list2.as<uint32_t>((size_t)count * len);  // each group has its own chain list
     XB_CUDA(cudaEventRecord(ss->fork, st));
     XB_CUDA(cudaStreamWaitEvent(ss->aux, ss->fork, 0));
-    verify_sequence(ops, p, b, ctx, ss->aux, own);
-    verify_sequence(ops, p, a, ctx, st, own);
+    if (tn.prep_split) {
+        // Each group's chains wait only for its own H_msg; the h_pre items
+        // of both groups run as one launch on a third stream, enqueued
+        // after the two H_msg launches so these get their CTAs first, and
+        // only the L-trees wait for it.
+        XB_CUDA(cudaStreamWaitEvent(ss->pre, ss->fork, 0));
+        ops->verify_prep_part(b, ctx, ss->aux, 1);
+        ops->verify_prep_part(a, ctx, st, 1);
+        ops->verify_prep_part(v, ctx, ss->pre, 2);
+        XB_CUDA(cudaEventRecord(ss->pre_done, ss->pre));
+        verify_sequence(ops, p, b, ctx, ss->aux, own, false, ss->pre_done);
+        verify_sequence(ops, p, a, ctx, st, own, false, ss->pre_done);
+    } else {
+        verify_sequence(ops, p, b, ctx, ss->aux, own);
+        verify_sequence(ops, p, a, ctx, st, own);
+    }
     XB_CUDA(cudaEventRecord(ss->join, ss->aux));
     XB_CUDA(cudaStreamWaitEvent(st, ss->join, 0));
 }

@@ -95,11 +95,14 @@ class PinnedBuf {
 };
 
 // Second stream of a split verify batch (the long-H_msg group runs there
-// while the short group runs on the caller's stream) and its fork / join.
+// while the short group runs on the caller's stream) and its fork / join;
+// a third stream for the h_pre items of both groups and the event that
+// ends them.
 struct SplitStreams {
-    cudaStream_t aux = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t aux = nullptr, pre = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, pre_done = nullptr;
     void create();
+    void destroy();
 };
 
 // Scratch of one in-flight launch sequence.  The engine owns one for its
@@ -187,7 +190,8 @@ class Engine {
     // groups whose L-tree runs with the GPU otherwise idle) instead of one
     // launch per level.
     void verify_sequence(const FamilyOps* ops, const xmss_params& p, const VerifyArgs& v, const void* ctx,
-                         cudaStream_t st, bool marks = true, bool fused_ltree = false);
+                         cudaStream_t st, bool marks = true, bool fused_ltree = false,
+                         cudaEvent_t hpre_ready = nullptr);
     // Single-sequence batches below this size are latency-bound: fused
     // L-tree (measured: it lowers serving latency at light load; for larger
     // batches, and for the tail group of a split batch, it cost throughput).

@@ -70,6 +70,19 @@ struct Launch {
         const uint64_t pre = (uint64_t)v.count * v.d * (F::LEN - 1 + v.tree_height);
         k_verify_prep<F><<<(unsigned)(hb + (pre + 63) / 64), 64, 0, st>>>(v, hb, (const Ctx*)ctx);
     }
+    static void verify_prep_part(const VerifyArgs& v, const void* ctx, cudaStream_t st, int part)
+    {
+        if (!v.count) return;
+        if (part == 1) {
+            const uint32_t hb = (v.count + 63) / 64;
+            k_verify_prep<F><<<hb, 64, 0, st>>>(v, hb, (const Ctx*)ctx);
+            return;
+        }
+        // the h_pre blocks alone (the chain kernels' pipe mix and 128-thread
+        // CTAs measured slower here)
+        const uint64_t pre = (uint64_t)v.count * v.d * (F::LEN - 1 + v.tree_height);
+        k_verify_prep<F><<<grid_for(pre, 64), 64, 0, st>>>(v, 0, (const Ctx*)ctx);
+    }
     static void verify_scatter(const VerifyArgs& v, uint32_t layer, cudaStream_t st)
     {
         const uint64_t items = (uint64_t)v.count * F::LEN;
@@ -138,6 +151,7 @@ struct Launch {
         o.hpre_bytes = sizeof(typename F::HPre);
         o.verify_partition = verify_partition;
         o.verify_prep = verify_prep;
+        o.verify_prep_part = verify_prep_part;
         o.verify_scatter = verify_scatter;
         o.verify_chains = verify_chains;
         o.verify_ltree = verify_ltree;

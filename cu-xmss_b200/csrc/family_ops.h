@@ -31,6 +31,8 @@ struct FamilyOps {
     void (*verify_partition)(const VerifyArgs& v, uint32_t blocks_max, uint32_t* sel_short, uint32_t* sel_long,
                              uint32_t* n2, cudaStream_t st);
     void (*verify_prep)(const VerifyArgs& v, const void* ctx, cudaStream_t st);
+    // one part of verify_prep: H_msg (part 1) or the h_pre items (part 2)
+    void (*verify_prep_part)(const VerifyArgs& v, const void* ctx, cudaStream_t st, int part);
     void (*verify_scatter)(const VerifyArgs& v, uint32_t layer, cudaStream_t st);
     void (*verify_chains)(const VerifyArgs& v, uint32_t layer, const void* ctx, cudaStream_t st);
     void (*verify_ltree)(const VerifyArgs& v, uint32_t layer, int cnt_in, uint32_t node_base, const uint8_t* src,
@@ -54,6 +56,7 @@ struct Tuning {
     uint32_t level_block = 128;         // L-tree and Merkle-level kernels
     uint32_t split_min = 1024;          // verify batches this large run as two groups ...
     uint32_t short_hmsg_blocks = 16;    // ... split at this many H_msg blocks
+    uint32_t prep_split = 1;            // split batches: h_pre in its own launch (1) or in each group's prep (0)
 };
 Tuning& tuning_for(unsigned func, unsigned n);
 

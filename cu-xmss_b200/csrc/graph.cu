@@ -31,9 +31,7 @@ struct xmss_b200_verify_graph {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (capture) cudaStreamDestroy(capture);
-        if (split.aux) cudaStreamDestroy(split.aux);
-        if (split.fork) cudaEventDestroy(split.fork);
-        if (split.join) cudaEventDestroy(split.join);
+        split.destroy();
     }
 };
 

@@ -4,7 +4,8 @@
 // The knobs are the CTA sizes of the chain kernels (verify; keygen and
 // sign), of the L-tree / Merkle-level kernels, and the split of large verify
 // batches into a short- and a long-H_msg group (the batch size from which
-// it applies, the H_msg length that separates the groups).  The tuner builds
+// it applies, the H_msg length that separates the groups, whether the
+// L-tree precomputation runs as a launch of its own).  The tuner builds
 // its own synthetic batch of the parameter set (seeded keys and signatures
 // of messages log-uniform in 32 B..4 KB, made by this library), times each
 // candidate with CUDA events (median of seven after a warm-up run, L2
@@ -52,6 +53,7 @@ void to_c(const xb::Tuning& t, xmss_b200_tuning* o)
     o->level_block = t.level_block;
     o->split_min = t.split_min;
     o->short_hmsg_blocks = t.short_hmsg_blocks;
+    o->prep_split = t.prep_split;
 }
 
 }  // namespace
@@ -66,7 +68,7 @@ extern "C" int xmss_b200_tuning_get(unsigned func, unsigned n, xmss_b200_tuning*
 extern "C" int xmss_b200_tuning_set(unsigned func, unsigned n, const xmss_b200_tuning* t)
 {
     if (!xb::family_ops(func, n) || !t || !block_ok(t->verify_chain_block) || !block_ok(t->keygen_chain_block) ||
-        !block_ok(t->level_block) || !t->split_min || !t->short_hmsg_blocks) {
+        !block_ok(t->level_block) || !t->split_min || !t->short_hmsg_blocks || t->prep_split > 1) {
         xb::set_last_error("xmss_b200_tuning_set: unknown family or shape out of range");
         return -1;
     }
@@ -77,6 +79,7 @@ extern "C" int xmss_b200_tuning_set(unsigned func, unsigned n, const xmss_b200_t
     d.level_block = t->level_block;
     d.split_min = t->split_min;
     d.short_hmsg_blocks = t->short_hmsg_blocks;
+    d.prep_split = t->prep_split;
     return 0;
 }
 
@@ -284,19 +287,28 @@ extern "C" int xmss_b200_autotune(uint32_t oid, int mt, uint32_t count, xmss_b20
                 tn.short_hmsg_blocks = keep_short;
             }
         }
+        // 5. where this batch splits: h_pre in its own launch or in each group's prep
+        if (count >= tn.split_min) {
+            const uint32_t keep = tn.prep_split;
+            const double cur_t = verify_ms();
+            note("prep_split", keep, cur_t, -1);
+            tn.prep_split = 1 - keep;
+            const double alt_t = verify_ms();
+            note("prep_split", tn.prep_split, alt_t, -1);
+            if (!(alt_t < kGain * cur_t)) tn.prep_split = keep;
+        }
         cudaEventDestroy(a);
         cudaEventDestroy(b);
         XB_CUDA(cudaStreamSynchronize(st));
-        cudaStreamDestroy(ss.aux);
-        cudaEventDestroy(ss.fork);
-        cudaEventDestroy(ss.join);
+        ss.destroy();
         xmss_b200_tuning bt;
         to_c(tn, &bt);
         if (best) *best = bt;
         snprintf(line, sizeof line,
                  "], \"best\": {\"verify_chain_block\": %u, \"keygen_chain_block\": %u, \"level_block\": %u, "
-                 "\"split_min\": %u, \"short_hmsg_blocks\": %u}}",
-                 bt.verify_chain_block, bt.keygen_chain_block, bt.level_block, bt.split_min, bt.short_hmsg_blocks);
+                 "\"split_min\": %u, \"short_hmsg_blocks\": %u, \"prep_split\": %u}}",
+                 bt.verify_chain_block, bt.keygen_chain_block, bt.level_block, bt.split_min, bt.short_hmsg_blocks,
+                 bt.prep_split);
         rep += line;
     } catch (const std::exception& ex) {
         xb::set_last_error(std::string("xmss_b200_autotune: ") + ex.what());

@@ -302,15 +302,53 @@ __device__ __forceinline__ void layer_addr(uint64_t idx, uint32_t th, uint32_t l
     tree = (th * (layer + 1) >= 64) ? 0 : idx >> (th * (layer + 1));
 }
 
+// h_pre of H node `pitem` of the signatures v selects: item = (signature,
+// layer, node), the nodes of a layer numbered L-tree level by level (level 0
+// pairs first), then the h authentication-path levels.  Reads the index
+// from the signature itself, so it runs independently of H_msg.
+template <class F>
+__device__ __forceinline__ void verify_hpre_item(const VerifyArgs& v, const typename F::Ctx* __restrict__ ctx,
+                                                 uint64_t pitem)
+{
+    using HPre = typename F::HPre;
+    const uint32_t nh = F::LEN - 1 + v.tree_height;
+    if (pitem >= (uint64_t)sel_count(v) * v.d * nh) return;
+    const uint32_t si = (uint32_t)(pitem / ((uint64_t)v.d * nh));
+    const uint32_t rem = (uint32_t)(pitem - (uint64_t)si * v.d * nh);
+    const uint32_t s = sel_sig(v, si);
+    const uint64_t item = (uint64_t)s * v.d * nh + rem;
+    const uint32_t layer = rem / nh;
+    uint32_t node = rem - layer * nh;
+    if (v.smlen[s] < v.sig_bytes) return;
+    const uint64_t idx = bytes_be(v.sm + v.sm_off[s], (int)v.index_bytes);
+    uint32_t leaf;
+    uint64_t tree;
+    layer_addr<F>(idx, v.tree_height, layer, leaf, tree);
+    uint32_t a[8];
+    if (node < F::LEN - 1) {
+        // locate (level, pair) of L-tree node `node`
+        int cnt = F::LEN, level = 0;
+        while (node >= (uint32_t)(cnt >> 1)) {
+            node -= cnt >> 1;
+            cnt = (cnt + 1) >> 1;
+            level++;
+        }
+        set_addr(a, layer, tree, ADDR_LTREE, leaf, (uint32_t)level, node);
+    } else {
+        const uint32_t i = node - (F::LEN - 1);
+        set_addr(a, layer, tree, ADDR_HASHTREE, 0, i, leaf >> (i + 1));
+    }
+    HPre hp;
+    F::h_pre(hp, ctx[v.key[s]], a);
+    ((HPre*)v.hpre)[item] = hp;
+}
+
 // Launch = [hmsg_blocks x 64 threads: one signature each] followed by
-// [pre blocks: one (signature, layer, H node) each].  The H nodes of a layer
-// are numbered L-tree level by level (level 0 pairs first), then the h
-// authentication-path levels.
+// [pre blocks: one H node's h_pre each]; either part may be empty.
 template <class F>
 __global__ void __launch_bounds__(64) k_verify_prep(VerifyArgs v, uint32_t hmsg_blocks_n,
                                                     const typename F::Ctx* __restrict__ ctx)
 {
-    using HPre = typename F::HPre;
     __shared__ uint32_t sh_hist[16];
     if (blockIdx.x < hmsg_blocks_n) {
         if (threadIdx.x < 16) sh_hist[threadIdx.x] = 0;
@@ -344,37 +382,7 @@ __global__ void __launch_bounds__(64) k_verify_prep(VerifyArgs v, uint32_t hmsg_
         flush_hist(sh_hist, v.hist);
         return;
     }
-    const uint32_t nh = F::LEN - 1 + v.tree_height;
-    const uint64_t pitem = (uint64_t)(blockIdx.x - hmsg_blocks_n) * blockDim.x + threadIdx.x;
-    if (pitem >= (uint64_t)sel_count(v) * v.d * nh) return;
-    const uint32_t si = (uint32_t)(pitem / ((uint64_t)v.d * nh));
-    const uint32_t rem = (uint32_t)(pitem - (uint64_t)si * v.d * nh);
-    const uint32_t s = sel_sig(v, si);
-    const uint64_t item = (uint64_t)s * v.d * nh + rem;
-    const uint32_t layer = rem / nh;
-    uint32_t node = rem - layer * nh;
-    if (v.smlen[s] < v.sig_bytes) return;
-    const uint64_t idx = bytes_be(v.sm + v.sm_off[s], (int)v.index_bytes);
-    uint32_t leaf;
-    uint64_t tree;
-    layer_addr<F>(idx, v.tree_height, layer, leaf, tree);
-    uint32_t a[8];
-    if (node < F::LEN - 1) {
-        // locate (level, pair) of L-tree node `node`
-        int cnt = F::LEN, level = 0;
-        while (node >= (uint32_t)(cnt >> 1)) {
-            node -= cnt >> 1;
-            cnt = (cnt + 1) >> 1;
-            level++;
-        }
-        set_addr(a, layer, tree, ADDR_LTREE, leaf, (uint32_t)level, node);
-    } else {
-        const uint32_t i = node - (F::LEN - 1);
-        set_addr(a, layer, tree, ADDR_HASHTREE, 0, i, leaf >> (i + 1));
-    }
-    HPre hp;
-    F::h_pre(hp, ctx[v.key[s]], a);
-    ((HPre*)v.hpre)[item] = hp;
+    verify_hpre_item<F>(v, ctx, (uint64_t)(blockIdx.x - hmsg_blocks_n) * blockDim.x + threadIdx.x);
 }
 
 // Splits the signatures into a short-H_msg group (at most `blocks_max` hash

@@ -121,7 +121,7 @@ class Tuning(C.Structure):
     """xmss_b200_tuning (include/xmss_b200.h)."""
 
     _fields_ = [(k, C.c_uint32) for k in ("verify_chain_block", "keygen_chain_block", "level_block", "split_min",
-                                          "short_hmsg_blocks")]
+                                          "short_hmsg_blocks", "prep_split")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -745,7 +745,9 @@ def tuning_get(func: int, n: int) -> dict:
 
 
 def tuning_set(func: int, n: int, shape: dict) -> None:
-    t = Tuning(**{k: int(shape[k]) for k, _ in Tuning._fields_})
+    """Sets the knobs `shape` names; the others keep their current values."""
+    cur = tuning_get(func, n)
+    t = Tuning(**{k: int(shape.get(k, cur[k])) for k, _ in Tuning._fields_})
     if lib.xmss_b200_tuning_set(func, n, C.byref(t)):
         raise ValueError(f"tuning_set({func}, {n}): {last_error()}")
 

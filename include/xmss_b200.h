@@ -103,15 +103,20 @@ void xmss_b200_verify_graph_destroy(xmss_b200_verify_graph *g);
  * threads) of the verify chain kernel, of the keygen / sign chain kernels
  * and of the L-tree / Merkle-level kernels, and the split of large verify
  * batches into a short- and a long-H_msg group on two streams (from
- * split_min signatures on, at short_hmsg_blocks hash blocks).  Results do
- * not depend on them.  Defaults: 128, 128, 128, 1024, 16.  Set them while no
- * call of that family runs (they are read at each launch). */
+ * split_min signatures on, at short_hmsg_blocks hash blocks).  In a split
+ * batch, prep_split = 1 runs the L-tree precomputation (h_pre) of both
+ * groups as a launch of its own on a third stream, so that each group's
+ * chains wait only for its H_msg; 0 runs it inside each group's prep
+ * launch.  Results do not depend on any of them.  Defaults: 128, 128, 128,
+ * 1024, 16, 1.  Set them while no call of that family runs (they are read
+ * at each launch). */
 typedef struct {
     uint32_t verify_chain_block;
     uint32_t keygen_chain_block;
     uint32_t level_block;
     uint32_t split_min;
     uint32_t short_hmsg_blocks;
+    uint32_t prep_split;
 } xmss_b200_tuning;
 
 int xmss_b200_tuning_get(unsigned int func, unsigned int n, xmss_b200_tuning *out);
