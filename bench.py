@@ -152,6 +152,23 @@ class ClockSampler:
 # replicas: every rank verifies its own batch, no data-path collective
 # ---------------------------------------------------------------------------
 
+def verify_launches(xb, count: int, wots_len: int = 67, layers: int = 1, func: int = 0, n: int = 32) -> int:
+    """Kernels of one device verify call (csrc/engine.cu Engine::verify): the
+    key contexts, then either one sequence (prep; per layer scatter, chains,
+    the L-tree levels or the one-launch warp L-tree below 256 signatures,
+    root) or the split into two such sequences after a partition launch,
+    with the prep as two H_msg launches and one h_pre launch when
+    prep_split is set."""
+    t = xb.tuning_get(func, n)
+    levels, c = 0, wots_len
+    while c > 1:
+        levels, c = levels + 1, (c + 1) // 2
+    if count < t["split_min"]:
+        return 1 + 1 + layers * (3 + (1 if count < 256 else levels))
+    per_group = layers * (3 + levels)
+    return 1 + 1 + (3 if t["prep_split"] else 2) + 2 * per_group
+
+
 def max_over_ranks(x: float, world: int, device) -> float:
     """The slowest rank's time (all ranks get it)."""
     if world <= 1:
@@ -382,7 +399,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "blocking_call_verifies_per_s": NUM_SIGS / blocking_s,
                 "api": "xmss_b200_sign_open_batch_async on two streams (pinned host buffers; copies of every "
                        "step inside the timed region, L2 flushed before each step)"},
-        "gpu_launches": 11 * args.steps,
+        "gpu_launches": verify_launches(xb, NUM_SIGS) * args.steps,
         "roofline": {"bound": "alu", "kernel": "k_verify_chains<Sha256N32>", "achieved": achieved,
                      "peak": probe_rate / 1e9, "unit": "Gcompr/s", "frac": achieved / (probe_rate / 1e9),
                      "traffic": traffic,

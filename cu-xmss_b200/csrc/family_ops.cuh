@@ -14,6 +14,29 @@ inline unsigned grid_for(uint64_t items, unsigned block = kBlock)
     return (unsigned)((items + block - 1) / block);
 }
 
+// Launch with programmatic stream serialization: the kernel starts launching
+// as the CTAs of the kernel before it in the stream exit and synchronises
+// with it through pdl_wait() (xmss_kernels.cuh).  A plain launch where the
+// attribute is refused (same results; only the overlap is lost).
+template <class... KArgs, class... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, kernel, args...) != cudaSuccess) {
+        (void)cudaGetLastError();
+        kernel<<<grid, block, 0, st>>>(args...);
+    }
+}
+
 // F runs every kernel except the chain kernels, which run FT (the same
 // family with another SHA-256 pipe mix; Ctx and HPre are shared).
 template <class F, class FT = F>
@@ -103,8 +126,14 @@ struct Launch {
         const uint64_t items = (uint64_t)v.count * ((cnt_in + 1) / 2);
         if (!items) return;
         const unsigned b = tune().level_block;
-        k_verify_ltree<F><<<grid_for(items, b), b, 0, st>>>(v, layer, cnt_in, node_base, src, src_stride, dst,
-                                                            dst_stride);
+        // the first level follows the chains (and, in a split batch, an
+        // event wait): a plain launch; later levels follow the level before
+        if (cnt_in == (int)F::LEN)
+            k_verify_ltree<F><<<grid_for(items, b), b, 0, st>>>(v, layer, cnt_in, node_base, src, src_stride, dst,
+                                                                dst_stride);
+        else
+            launch_pdl(k_verify_ltree<F>, grid_for(items, b), b, st, v, layer, cnt_in, node_base, src, src_stride,
+                       dst, dst_stride);
     }
     static void verify_ltree_warp(const VerifyArgs& v, uint32_t layer, cudaStream_t st)
     {
@@ -114,7 +143,7 @@ struct Launch {
     static void verify_root(const VerifyArgs& v, uint32_t layer, cudaStream_t st)
     {
         if (!v.count) return;
-        k_verify_root<F><<<(v.count + 63) / 64, 64, 0, st>>>(v, layer);
+        launch_pdl(k_verify_root<F>, (v.count + 63) / 64, 64, st, v, layer);
     }
     static void sign_prep(const SignArgs& g, const void* ctx, cudaStream_t st)
     {
