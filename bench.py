@@ -11,9 +11,11 @@ own batched keygen / sign (untimed) and the accept bitmap is checked.
 value      verifies/s with inputs resident in HBM, CUDA events around each
            step on the launching stream, L2 flushed between steps (the input
            is 14 MB, smaller than L2), max over ranks (replicas, weak scaling);
-           the steps run once as launches of xmss_b200_sign_open_device and
-           once as replays of its CUDA graph (xmss_b200_verify_graph_*), and
-           the faster is the value (both are reported in config)
+           the steps run once as launches of xmss_b200_sign_open_device,
+           once as replays of its CUDA graph (xmss_b200_verify_graph_*) and
+           once as the one-launch persistent form fed by a device work queue
+           (xmss_b200_sign_open_device_persistent); the fastest is the value
+           (all three are reported in config)
 e2e        the same through the host-buffer C-ABI from pinned host memory,
            every step's copies included: xmss_b200_sign_open_batch_async on
            two streams in turn (one step's copies overlap the other's
@@ -272,10 +274,42 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     correct = correct and bool((d_status.cpu().numpy() == w["expect"]).all())
     graph.close()
     t_ms_graph = max_over_ranks(float(sum(s.elapsed_time(e) for s, e in zip(starts, ends))), world, dev)
-    launch_mode = "cuda_graph" if t_ms_graph < t_ms_stream else "stream"
-    if launch_mode == "cuda_graph":
-        clocks = gclocks
-    t_ms = min(t_ms_graph, t_ms_stream)
+
+    # ---- the same steps as one persistent launch each (device work queue) ----
+    def verify_persistent():
+        xb.sign_open_device_persistent(OID, False, NUM_SIGS, d_sm.data_ptr(), d_off.data_ptr(), d_len.data_ptr(),
+                                       d_pk.data_ptr(), NUM_KEYS, d_kix.data_ptr(), d_status.data_ptr(), sh)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        verify_persistent()
+    torch.cuda.synchronize()
+    d_status.fill_(7)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as pclocks:
+        for i in range(args.steps):
+            flush.zero_()
+            starts[i].record(stream)
+            verify_persistent()
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    persist_ok = bool((d_status.cpu().numpy() == w["expect"]).all())
+    if not persist_ok:
+        log(f"rank {rank}: persistent form: accept bitmap mismatch")
+    correct = correct and persist_ok
+    t_ms_persist = max_over_ranks(float(sum(s.elapsed_time(e) for s, e in zip(starts, ends))), world, dev)
+
+    forms = {"stream": (t_ms_stream, clocks, verify_launches(xb, NUM_SIGS)),
+             "cuda_graph": (t_ms_graph, gclocks, verify_launches(xb, NUM_SIGS)),
+             "persistent": (t_ms_persist, pclocks, 1)}
+    if not persist_ok:
+        del forms["persistent"]
+    launch_mode = min(forms, key=lambda k: forms[k][0])
+    t_ms, clocks, launches_per_step = forms[launch_mode]
     value = replica_rate(NUM_SIGS, world, args.steps, t_ms / 1e3)
 
     # ---- per-kernel timing (separate pass; profiling serialises calls) ----
@@ -393,13 +427,14 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                    "l2": "flushed between steps (512 MB write; inputs 14 MB < 126 MB L2)",
                    "launch": launch_mode,
                    "ms_per_step_stream_launches": t_ms_stream / args.steps,
-                   "ms_per_step_cuda_graph": t_ms_graph / args.steps},
+                   "ms_per_step_cuda_graph": t_ms_graph / args.steps,
+                   "ms_per_step_persistent": t_ms_persist / args.steps},
         "correct": correct,
         "e2e": {"value": e2e_value, "unit": "verifies/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "blocking_call_verifies_per_s": NUM_SIGS / blocking_s,
                 "api": "xmss_b200_sign_open_batch_async on two streams (pinned host buffers; copies of every "
                        "step inside the timed region, L2 flushed before each step)"},
-        "gpu_launches": verify_launches(xb, NUM_SIGS) * args.steps,
+        "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "alu", "kernel": "k_verify_chains<Sha256N32>", "achieved": achieved,
                      "peak": probe_rate / 1e9, "unit": "Gcompr/s", "frac": achieved / (probe_rate / 1e9),
                      "traffic": traffic,

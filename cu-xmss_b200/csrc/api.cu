@@ -582,6 +582,24 @@ extern "C" int xmss_b200_sign_open_device(uint32_t oid, int mt, uint32_t count, 
     });
 }
 
+extern "C" int xmss_b200_sign_open_device_persistent(uint32_t oid, int mt, uint32_t count, const uint8_t* d_sm,
+                                                     const uint64_t* d_sm_off, const uint64_t* d_smlen,
+                                                     const uint8_t* d_pk, uint32_t npk, const uint32_t* d_pk_index,
+                                                     int* d_status, void* stream)
+{
+    xmss_params p;
+    if (parse(&p, oid, mt)) return kBad;
+    if (count && (!d_pk_index || !npk)) return kBad;
+    return guarded([&](Engine& e) {
+        const xb::FamilyOps* ops = xb::ops_for(p);
+        cudaStream_t st = (cudaStream_t)stream;
+        e.begin(st);
+        e.verify_persistent(ops, p, count, d_sm, d_sm_off, d_smlen, d_pk, npk, d_pk_index, d_status, st);
+        e.end(st);
+        return kOk;
+    });
+}
+
 extern "C" int xmss_b200_sign_batch(int mt, uint32_t count, uint8_t* sk, const uint8_t* msgs,
                                     const uint64_t* m_off, const uint64_t* mlen, uint8_t* sm,
                                     const uint64_t* sm_off, uint64_t* smlen, int* ret)

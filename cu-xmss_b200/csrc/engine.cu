@@ -8,6 +8,7 @@
 #include <map>
 #include <tuple>
 
+#include "verify_persist.cuh"
 #include "xmss_kernels.cuh"
 
 namespace xb {
@@ -71,7 +72,7 @@ void SplitStreams::destroy()
 void Workspace::order_on(cudaStream_t st)
 {
     for (DevBuf* b : {&ctx, &jobs, &refs, &wpk, &wpk2, &nodes, &keys, &node, &lens, &idx, &leaf, &hpre, &hist, &list,
-                      &list2, &aux, &work})
+                      &list2, &aux, &work, &pstate})
         b->order_on(st);
 }
 
@@ -453,6 +454,59 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
     }
     XB_CUDA(cudaEventRecord(ss->join, ss->aux));
     XB_CUDA(cudaStreamWaitEvent(st, ss->join, 0));
+}
+
+void Engine::verify_persistent(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_sm,
+                               const uint64_t* d_sm_off, const uint64_t* d_smlen, const uint8_t* d_pk, uint32_t npk,
+                               const uint32_t* d_pk_index, int* d_status, cudaStream_t st)
+{
+    Workspace& w = ws_;
+    XB_CUDA(cudaMemsetAsync(work_, 0, 3 * sizeof(unsigned long long), st));
+    if (!count) return;
+    const uint32_t n = p.n, len = ops->len, d = p.d, nh = len - 1 + p.tree_height;
+    const uint32_t groups = (count + 31) / 32;
+    VerifyArgs v{};
+    v.sm = d_sm;
+    v.sm_off = d_sm_off;
+    v.smlen = d_smlen;
+    v.key = d_pk_index;
+    v.key_root = d_pk;
+    v.key_stride = 2 * n;
+    v.node = w.node.as<uint8_t>((size_t)count * n);
+    v.lens = w.lens.as<uint8_t>((size_t)count * len);
+    v.idx = w.idx.as<uint64_t>(count);
+    v.status = d_status;
+    v.wpk = w.wpk.as<uint8_t>((size_t)count * len * n);
+    v.wpk2 = w.wpk2.as<uint8_t>((size_t)count * ((len + 1) / 2) * n);
+    v.leaf = w.leaf.as<uint8_t>((size_t)count * n);
+    v.hpre = w.hpre.get((size_t)count * d * nh * ops->hpre_bytes);
+    v.work = work_;
+    v.count = count;
+    v.index_bytes = p.index_bytes;
+    v.sig_bytes = p.sig_bytes;
+    v.tree_height = p.tree_height;
+    v.d = d;
+    // state: ticket (8 B), header, then per (group, layer) ready / ntot /
+    // chains_done / 8 L-tree level counters, then per group h_pre counters
+    const size_t gl = (size_t)groups * d;
+    const size_t words = 4 + gl * 11 + groups;
+    uint8_t* st8 = w.pstate.as<uint8_t>(8 + words * 4);
+    uint32_t* u = (uint32_t*)(st8 + 8);
+    PersistArgs q{};
+    q.ticket = (unsigned long long*)st8;
+    q.hdr = u;
+    q.ready = u + 4;
+    q.ntot = q.ready + gl;
+    q.chains_done = q.ntot + gl;
+    q.lt_done = q.chains_done + gl;
+    q.hpre_done = q.lt_done + 8 * gl;
+    q.list = w.list.as<uint32_t>((size_t)groups * 32 * len);
+    q.ctx = w.ctx.get((size_t)npk * ops->ctx_bytes);
+    q.npk = npk;
+    q.groups = groups;
+    XB_CUDA(cudaMemsetAsync(st8, 0, 8 + words * 4, st));
+    ops->verify_persist(v, q, st);
+    XB_CUDA(cudaGetLastError());
 }
 
 void Engine::last_verify_work(unsigned long long out[3])

@@ -110,7 +110,8 @@ struct SplitStreams {
 // batches on different streams never share intermediate buffers.
 struct Workspace {
     DevBuf ctx, jobs, refs, wpk, wpk2, nodes, keys, node, lens, idx, leaf, hpre, hist, list, list2, aux;
-    DevBuf work;  // verify work counters of non-engine workspaces
+    DevBuf work;    // verify work counters of non-engine workspaces
+    DevBuf pstate;  // task counters of the persistent verify
     PinnedBuf h_jobs;
     void order_on(cudaStream_t st);  // every buffer grows stream-ordered on st
     // Streams of large verify batches (two groups split by H_msg length)
@@ -156,6 +157,13 @@ class Engine {
     void verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_sm,
                 const uint64_t* d_sm_off, const uint64_t* d_smlen, const uint8_t* d_pk, uint32_t npk,
                 const uint32_t* d_pk_index, int* d_status, cudaStream_t st, Workspace& w, bool allow_split);
+
+    // The same verify as one persistent launch fed by a device work queue
+    // (verify_persist.cuh), on st only; same statuses, plus -3 for every
+    // signature if a dependency wait ran out.
+    void verify_persistent(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_sm,
+                           const uint64_t* d_sm_off, const uint64_t* d_smlen, const uint8_t* d_pk, uint32_t npk,
+                           const uint32_t* d_pk_index, int* d_status, cudaStream_t st);
 
     // Key generation from seeds (count x 3n) into pk (count x 2n) and sk
     // (count x sk_bytes), no OID prefix.

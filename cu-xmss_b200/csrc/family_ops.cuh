@@ -3,6 +3,7 @@
 #pragma once
 
 #include "family_ops.h"
+#include "verify_persist.cuh"
 #include "xmss_kernels.cuh"
 
 namespace xb {
@@ -145,6 +146,20 @@ struct Launch {
         if (!v.count) return;
         launch_pdl(k_verify_root<F>, (v.count + 63) / 64, 64, st, v, layer);
     }
+    static void verify_persist(const VerifyArgs& v, const PersistArgs& q, cudaStream_t st)
+    {
+        if (!v.count) return;
+        // as many CTAs as fit on the GPU at once: each loops over the ticket
+        // sequence (more would only queue behind them; fewer leave SMs idle)
+        static const unsigned grid = [] {
+            int dev = 0, sms = 0, per = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_verify_persist<F, FT>, 128, 0);
+            return (unsigned)(sms * (per > 0 ? per : 1));
+        }();
+        k_verify_persist<F, FT><<<grid, 128, 0, st>>>(v, q);
+    }
     static void sign_prep(const SignArgs& g, const void* ctx, cudaStream_t st)
     {
         if (!g.count) return;
@@ -186,6 +201,7 @@ struct Launch {
         o.verify_ltree = verify_ltree;
         o.verify_root = verify_root;
         o.verify_ltree_warp = verify_ltree_warp;
+        o.verify_persist = verify_persist;
         o.sign_prep = sign_prep;
         o.sign_chains = sign_chains;
         o.core_hash = core_hash;

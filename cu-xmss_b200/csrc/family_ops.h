@@ -13,6 +13,7 @@ struct LeafRef;
 struct TreeJob;
 struct VerifyArgs;
 struct SignArgs;
+struct PersistArgs;
 
 struct FamilyOps {
     const char* name;
@@ -39,6 +40,8 @@ struct FamilyOps {
                          uint32_t src_stride, uint8_t* dst, uint32_t dst_stride, cudaStream_t st);
     void (*verify_root)(const VerifyArgs& v, uint32_t layer, cudaStream_t st);
     void (*verify_ltree_warp)(const VerifyArgs& v, uint32_t layer, cudaStream_t st);  // whole L-tree, warp / sig
+    // the whole verify (every layer) as one persistent launch (verify_persist.cuh)
+    void (*verify_persist)(const VerifyArgs& v, const PersistArgs& q, cudaStream_t st);
     void (*sign_prep)(const SignArgs& g, const void* ctx, cudaStream_t st);
     void (*sign_chains)(const SignArgs& g, const void* ctx, cudaStream_t st);
     void (*core_hash)(const uint8_t* msgs, const uint64_t* off, const uint64_t* len, uint32_t count, uint8_t* out,

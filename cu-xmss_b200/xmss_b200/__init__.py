@@ -135,6 +135,7 @@ lib.xmss_b200_sign_batch.argtypes = [C.c_int, C.c_uint32, _u8p, _u8p, _u64p, _u6
 lib.xmss_b200_core_hash_batch.argtypes = [C.c_uint, C.c_uint, C.c_uint32, _u8p, _u64p, _u64p, _u8p]
 lib.xmss_b200_last_verify_work.argtypes = [C.POINTER(Work)]
 lib.xmss_b200_sign_open_device_noalloc.argtypes = lib.xmss_b200_sign_open_device.argtypes
+lib.xmss_b200_sign_open_device_persistent.argtypes = lib.xmss_b200_sign_open_device.argtypes
 lib.xmss_b200_profile.argtypes = [C.c_int]
 lib.xmss_b200_phase_ms.argtypes = [C.POINTER(C.c_double)]
 lib.xmss_b200_rate_probe.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
@@ -542,6 +543,16 @@ def sign_open_device(oid: int, mt: bool, count: int, d_sm: int, d_sm_off: int, d
                                               d_status, stream), "sign_open_device")
     if r:
         raise ValueError(f"sign_open_device returned {r}: {last_error()}")
+
+
+def sign_open_device_persistent(oid: int, mt: bool, count: int, d_sm: int, d_sm_off: int, d_smlen: int, d_pk: int,
+                                npk: int, d_pk_index: int, d_status: int, stream: int = 0) -> None:
+    """xmss_b200_sign_open_device_persistent: sign_open_device as one
+    persistent launch fed by a device work queue."""
+    r = _check(lib.xmss_b200_sign_open_device_persistent(oid, int(mt), count, d_sm, d_sm_off, d_smlen, d_pk, npk,
+                                                         d_pk_index, d_status, stream), "sign_open_device_persistent")
+    if r:
+        raise ValueError(f"sign_open_device_persistent returned {r}: {last_error()}")
 
 
 def sign_open_device_noalloc(oid: int, mt: bool, count: int, d_sm: int, d_sm_off: int, d_smlen: int, d_pk: int,

@@ -69,6 +69,20 @@ int xmss_b200_sign_open_device(uint32_t oid, int mt, uint32_t count, const uint8
                                const uint8_t *d_pk, uint32_t npk, const uint32_t *d_pk_index,
                                int *d_status, void *stream);
 
+/* Persistent form of xmss_b200_sign_open_device (same arguments, same
+ * statuses): the whole batch, every XMSS^MT layer included, runs as ONE
+ * kernel launch whose warps take tasks from a device work queue (a ticket
+ * counter over key contexts, H_msg, L-tree precomputation, WOTS chains
+ * bucketed longest first, L-tree levels and compute_root, in dependency
+ * order).  Every dependency wait inside the launch is bounded; if one runs
+ * out (a single H_msg taking seconds, i.e. a message of hundreds of MB)
+ * every status of the batch is -3.  Replaces, like xmss_b200_sign_open_device,
+ * a loop of xmss[mt]_sign_open calls (xmss.c:45-60, 95-109). */
+int xmss_b200_sign_open_device_persistent(uint32_t oid, int mt, uint32_t count, const uint8_t *d_sm,
+                                          const uint64_t *d_sm_off, const uint64_t *d_smlen,
+                                          const uint8_t *d_pk, uint32_t npk, const uint32_t *d_pk_index,
+                                          int *d_status, void *stream);
+
 /* Pipelined form of xmss_b200_sign_open_batch: enqueues the copy of the
  * signed messages from the caller's memory, the verify, and the copy of the
  * statuses into `status` on `stream` (cudaStream_t as void*) and returns.
