@@ -99,6 +99,13 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p)
     return x;
 }
 
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p)
+{
+    uint32_t x;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(x) : "l"(p) : "memory");
+    return x;
+}
+
 __device__ __forceinline__ unsigned long long global_ns()
 {
     unsigned long long t;
@@ -107,14 +114,16 @@ __device__ __forceinline__ unsigned long long global_ns()
 }
 
 // Every lane polls until *c >= target.  Warp-uniform result: false when the
-// wait ran out (the error flag is then set) or another warp failed.
+// wait ran out (the error flag is then set) or another warp failed.  Polls
+// are relaxed loads followed by one acquire fence, so a waiting warp does not
+// order its SM's L1 against the GPU on every poll.
 __device__ __forceinline__ bool persist_wait(const uint32_t* c, uint32_t target, uint32_t* err)
 {
     bool ok = true;
     if (ld_acquire(c) < target) {
         const unsigned long long t0 = global_ns();
         unsigned ns = 64;
-        while (ld_acquire(c) < target) {
+        while (ld_relaxed(c) < target) {
             if (*(volatile uint32_t*)err) {
                 ok = false;
                 break;
@@ -127,6 +136,7 @@ __device__ __forceinline__ bool persist_wait(const uint32_t* c, uint32_t target,
             __nanosleep(ns);
             if (ns < 1024) ns *= 2;
         }
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
     }
     return __all_sync(0xffffffffu, ok);
 }
@@ -304,7 +314,12 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
                 uint32_t x[F::NW], a[8];
                 F::load(x, sig + (uint64_t)chain * F::N);
                 set_addr(a, layer, tree, ADDR_OTS, leafidx, chain, 0);
-                run_chain<FT>(x, ((const typename FT::Ctx*)ctx)[v.key[s]], a, start, 15 - start, false);
+                // the key context in registers: ctx is written by this launch, so
+                // the chain loop cannot read it through the read-only path, and
+                // re-reading its midstate from L1 / L2 on every F call made a
+                // lone chain warp ~3x slower than in k_verify_chains
+                const typename FT::Ctx kc = ((const typename FT::Ctx*)ctx)[v.key[s]];
+                run_chain<FT>(x, kc, a, start, 15 - start, false);
                 F::store(v.wpk + (uint64_t)item * F::N, x);
             }
             persist_signal(&q.chains_done[gl]);
