@@ -25,10 +25,18 @@ roofline   the chain kernel (the dominant kernel): algorithmic SHA-256
            compressions per launch (4 per F call, counted on the GPU) over
            its CUDA-event duration, against the measured compression rate of
            the rate probe (same SHA-256 core, all SMs busy) in the same run
-secondary  XMSS-SHA2_16_256 keygen leaves/s (8 keys, 65,536 leaves each)
---impl reference   times the reference's own CPU path (oracle/_ref, compiled
-           from the reference sources) on a bounded sample of the same
-           workload on all host cores.
+secondary  (N = 1) keygen: 8 x XMSS-SHA2_16_256 + 1 x XMSS-SHA2_20_256
+           leaves/s, median of 3, every public key compared with the golden
+           keys of the same seeds; mix: XMSS^MT 20/2 and 40/4, SHA-512 and
+           SHAKE128 sets, 2,048 signs at consecutive indices and verifies
+           each, signatures compared with the oracle's digests; serve: a
+           short Poisson sweep of the serving loop (p50 / p99, sustained rate
+           at p99 sign <= 10 ms, against the plain per-call path), burst
+           signatures signed again by the oracle
+--impl reference   times the reference's own CPU verify (xmss_sign_open of
+           the reference C path compiled into oracle/_ref) on all host cores
+           over the same 4,096 signed messages (built byte for byte by the
+           CPU oracle: no GPU code runs in that arm), with the same config.
 """
 from __future__ import annotations
 
@@ -50,6 +58,7 @@ NUM_KEYS = 64
 OID = 0x01  # XMSS-SHA2_10_256
 SEED = 20260303
 MEASURED = os.path.join(ROOT, "MEASURED_PEAKS.json")
+METRIC = "XMSS-SHA2_10_256 batched verifies/s (4096 sigs, 64 keys, mlen 32B-4KB log-uniform, 10% bit-flipped)"
 
 
 def log(*a):
@@ -60,34 +69,93 @@ def log(*a):
 # workload
 # ---------------------------------------------------------------------------
 
-def make_workload(xb, rank: int = 0):
-    """Seeded config: keys, signed messages (10% one-bit corrupted)."""
-    rng = np.random.default_rng(SEED + rank)
-    p = xb.parse_oid(OID)
-    seeds = np.frombuffer(rng.bytes(NUM_KEYS * 3 * p.n), np.uint8).reshape(NUM_KEYS, 3 * p.n)
-    pks, sks = xb.keypair_batch(OID, False, seeds)
-    keyix = rng.integers(0, NUM_KEYS, NUM_SIGS).astype(np.uint32)
-    idx = rng.integers(0, 1 << p.full_height, NUM_SIGS)
-    mlen = np.exp(rng.uniform(np.log(32), np.log(4096), NUM_SIGS)).astype(np.int64)
+def _workload_draws(rng, n: int, full_height: int, count: int, keys: int):
+    """The seeded random inputs of the verify workload, in draw order."""
+    seeds = np.frombuffer(rng.bytes(keys * 3 * n), np.uint8).reshape(keys, 3 * n)
+    keyix = rng.integers(0, keys, count).astype(np.uint32)
+    idx = rng.integers(0, 1 << full_height, count)
+    mlen = np.exp(rng.uniform(np.log(32), np.log(4096), count)).astype(np.int64)
     msgs = [rng.bytes(int(L)) for L in mlen]
-    rows = np.array(sks[keyix])
-    for i in range(NUM_SIGS):
-        rows[i, 4:4 + p.index_bytes] = np.frombuffer(int(idx[i]).to_bytes(p.index_bytes, "big"), np.uint8)
-    ret, sms = xb.sign_batch(False, rows, msgs)
-    assert (ret == 0).all()
-    flip = rng.choice(NUM_SIGS, NUM_SIGS // 10, replace=False)
-    # Index 2^h - 1 is the reference's exhaustion case (xmss_core.c:212-231):
-    # the key is wiped before signing, so that signature must reject.
-    expect = np.where(idx == (1 << p.full_height) - 1, -1, 0).astype(np.int32)
+    return seeds, keyix, idx, mlen, msgs
+
+
+def _corrupt(rng, sms, idx, full_height: int, count: int):
+    """10% of the signed messages get one bit flipped; index 2^h - 1 is the
+    reference's exhaustion case (xmss_core.c:212-231): the key is wiped
+    before signing, so that signature must reject too."""
+    flip = rng.choice(count, count // 10, replace=False)
+    expect = np.where(idx == (1 << full_height) - 1, -1, 0).astype(np.int32)
     sms = [bytearray(s) for s in sms]
     for i in flip:
         pos = int(rng.integers(0, len(sms[i])))
         sms[i][pos] ^= 1 << int(rng.integers(0, 8))
         expect[i] = -1
-    sms = [bytes(s) for s in sms]
+    return [bytes(s) for s in sms], expect
+
+
+def make_workload(xb, rank: int = 0, count: int = NUM_SIGS, keys: int = NUM_KEYS):
+    """Seeded config: keys, signed messages (10% one-bit corrupted), made by
+    this library's batched keygen and sign."""
+    rng = np.random.default_rng(SEED + rank)
+    p = xb.parse_oid(OID)
+    seeds, keyix, idx, mlen, msgs = _workload_draws(rng, p.n, p.full_height, count, keys)
+    pks, sks = xb.keypair_batch(OID, False, seeds)
+    rows = np.array(sks[keyix])
+    for i in range(count):
+        rows[i, 4:4 + p.index_bytes] = np.frombuffer(int(idx[i]).to_bytes(p.index_bytes, "big"), np.uint8)
+    ret, sms = xb.sign_batch(False, rows, msgs)
+    assert (ret == 0).all()
+    sms, expect = _corrupt(rng, sms, idx, p.full_height, count)
     buf, off, ln = xb.pack(sms, align=16)
     return dict(p=p, pks=pks, keyix=keyix, sms=sms, buf=buf, off=off, len=ln, expect=expect,
                 mean_mlen=float(mlen.mean()))
+
+
+def make_workload_cpu(rank: int = 0, count: int = NUM_SIGS, keys: int = NUM_KEYS):
+    """The same workload as make_workload, byte for byte, built on the host
+    cores by the CPU oracle (no GPU code runs): the reference arm's inputs.
+    Each key's tree is built once on all cores; the signatures at the last
+    index are made from the tree of the wiped (all-zero) key, as the
+    reference signs them (xmss_core.c:212-231)."""
+    from concurrent.futures import ThreadPoolExecutor as Pool
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+
+    o = Oracle()
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(SEED + rank)
+    p = o.params(OID)
+    n = p.n
+    seeds, keyix, idx, mlen, msgs = _workload_draws(rng, n, p.full_height, count, keys)
+    seeds = [s.tobytes() for s in seeds]
+    trees = [o.tree_nodes(p, s[:n], s[2 * n:], 0, 0, cores) for s in seeds]
+    last = (1 << p.full_height) - 1
+    wiped = o.tree_nodes(p, bytes(n), bytes(n), 0, 0, cores) if (idx == last).any() else None
+    oidb = OID.to_bytes(4, "big")
+    pks = np.stack([np.frombuffer(oidb + t[-n:] + s[2 * n:], np.uint8) for t, s in zip(trees, seeds)])
+
+    def sign(i):
+        k = int(keyix[i])
+        s = seeds[k]
+        sk = int(idx[i]).to_bytes(p.index_bytes, "big") + s[:2 * n] + trees[k][-n:] + s[2 * n:]
+        r, _, sm = o.sign(p, sk, msgs[i], trees=wiped if idx[i] == last else trees[k])
+        assert r == 0
+        return sm
+
+    with Pool(cores) as ex:  # the oracle's ctypes calls release the GIL
+        sms = list(ex.map(sign, range(count)))
+    sms, expect = _corrupt(rng, sms, idx, p.full_height, count)
+    return dict(p=p, pks=pks, keyix=keyix, sms=sms, expect=expect, mean_mlen=float(mlen.mean()))
+
+
+def workload_config(w: dict, world: int) -> dict:
+    """The `config` of both arms' lines: the workload only, identical in the
+    two arms (how each arm runs it is reported beside it)."""
+    return {"workload": "batched verify, XMSS-SHA2_10_256", "oid": OID, "signatures": len(w["sms"]),
+            "keys": int(w["pks"].shape[0]), "mlen": "log-uniform 32..4096 B", "mean_mlen": w["mean_mlen"],
+            "bitflip_fraction": 0.1, "parallelism": f"replicas x{world}",
+            "l2": "GPU arm: flushed between steps (512 MB write; inputs 14 MB < 126 MB L2)"}
 
 
 # ---------------------------------------------------------------------------
@@ -391,10 +459,18 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     h2d = int(w["buf"].nbytes + h_off.nbytes + h_len.nbytes + NUM_KEYS * 2 * n + h_kix.nbytes)
     d2h = 4 * NUM_SIGS
 
-    # ---- secondary: keygen leaves/s (XMSS-SHA2_16_256) ----
-    sec = None
-    if not args.skip_keygen:
-        sec = keygen_rate(xb, torch, dev, sh)
+    # ---- secondaries at N = 1: keygen (config 3), the XMSS^MT / wide-hash
+    # mix (config 4) and a short serving sweep (config 5) ----
+    sec = {}
+    if world == 1 and not args.skip_keygen:
+        sec["keygen"] = keygen_rate(xb, torch, dev, sh)
+    if world == 1 and not args.skip_mix:
+        sec["mix"] = mix_rates(xb, torch, dev, sh)
+    if world == 1 and not args.skip_serve:
+        sargs = argparse.Namespace(**vars(args))
+        sargs.serve_rates, sargs.serve_n, sargs.serve_seconds = args.sec_serve_rates, 30000, 1.0
+        sargs.serve_plain_n, sargs.serve_check = 60, 1
+        sec["serve"] = run_serve(sargs)
 
     # ---- CPU baseline (rank 0, N = 1) ----
     cpu = None
@@ -409,7 +485,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     pipeline_rate = comp_total / (t_ms / args.steps / 1e3) / 1e9 if world == 1 else None
     traffic = read_traffic()
     out = {
-        "metric": "XMSS-SHA2_10_256 batched verifies/s (4096 sigs, 64 keys, mlen 32B-4KB log-uniform, 10% bit-flipped)",
+        "metric": METRIC,
         "value": value,
         "unit": "verifies/s",
         "n_gpus": world,
@@ -421,11 +497,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic (seeded keys and messages; signatures made by this library, accept bitmap checked)",
-        "config": {"workload": "batched verify, XMSS-SHA2_10_256", "oid": OID, "signatures": NUM_SIGS,
-                   "keys": NUM_KEYS, "mlen": "log-uniform 32..4096 B", "mean_mlen": w["mean_mlen"],
-                   "bitflip_fraction": 0.1, "parallelism": f"replicas x{world}",
-                   "l2": "flushed between steps (512 MB write; inputs 14 MB < 126 MB L2)",
-                   "launch": launch_mode,
+        "config": workload_config(w, world),
+        "launch": {"form": launch_mode,
                    "ms_per_step_stream_launches": t_ms_stream / args.steps,
                    "ms_per_step_cuda_graph": t_ms_graph / args.steps,
                    "ms_per_step_persistent": t_ms_persist / args.steps},
@@ -438,6 +511,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "roofline": {"bound": "alu", "kernel": "k_verify_chains<Sha256N32>", "achieved": achieved,
                      "peak": probe_rate / 1e9, "unit": "Gcompr/s", "frac": achieved / (probe_rate / 1e9),
                      "traffic": traffic,
+                     "traffic_source": "not measured in this run: dram__bytes_read.sum + dram__bytes_write.sum of "
+                                       "one launch of this kernel on this workload, read from the committed ncu "
+                                       "summary profiles/verify_chains_sha256_4096sigs.md",
                      "peak_source": "measured in this run: rate probe, 4 x 148 x 16 CTAs of 128 threads x "
                                     f"{iters} SHA-256 compressions (same core as the kernels), best of the "
                                     "ALU-pipe and FMA-pipe forms",
@@ -453,20 +529,37 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     }
     if sec:
         out["secondary"] = sec
+        out["correct_secondary"] = all(s.get("correct") is not False for s in sec.values())
     if cpu:
         out["cpu_baseline"] = cpu
     return out
 
 
-def keygen_rate(xb, torch, dev, sh, sets=((0x02, 8), (0x03, 1))):
+KEYGEN_SETS = ((0x02, 8), (0x03, 1))  # 8 x XMSS-SHA2_16_256 + 1 x XMSS-SHA2_20_256 (n = 32)
+KEYGEN_GOLDEN = os.path.join(ROOT, "tests", "golden", "keygen_config3.json")
+
+
+def keygen_seeds(sets=KEYGEN_SETS, n: int = 32):
+    """The seeded 96-byte seeds of the batched-keygen workload, per (oid,
+    count): count x 3n bytes (SK_SEED || SK_PRF || PUB_SEED).  The golden
+    public keys (tests/golden/keygen_config3.json) are made from the same
+    seeds by tests/golden/make_keygen_golden.py."""
+    rng = np.random.default_rng(SEED + 16)
+    return [(oid, np.frombuffer(rng.bytes(count * 3 * n), np.uint8).reshape(count, 3 * n).copy())
+            for oid, count in sets]
+
+
+def keygen_rate(xb, torch, dev, sh, sets=KEYGEN_SETS, repeats: int = 3):
     """Batched keygen of config 3: 8 XMSS-SHA2_16_256 keys and 1
     XMSS-SHA2_20_256 key from seeded seeds, in one timed region (`sets`
-    other (oid, keys) pairs, e.g. one h=16 key for a profiler capture)."""
-    rng = np.random.default_rng(SEED + 16)
+    other (oid, keys) pairs, e.g. one h=16 key for a profiler capture),
+    timed `repeats` times; the public keys are compared with the committed
+    golden keys of the same seeds."""
     jobs = []
-    for oid, count in sets:
+    for oid, seeds_np in keygen_seeds(sets):
         p = xb.parse_oid(oid)
-        seeds = torch.from_numpy(np.frombuffer(rng.bytes(count * 3 * p.n), np.uint8).copy()).to(dev)
+        count = seeds_np.shape[0]
+        seeds = torch.from_numpy(seeds_np.reshape(-1)).to(dev)
         d_pk = torch.empty(count * 2 * p.n, dtype=torch.uint8, device=dev)
         d_sk = torch.empty(count * p.sk_bytes, dtype=torch.uint8, device=dev)
         jobs.append((oid, count, p, seeds, d_pk, d_sk))
@@ -477,19 +570,43 @@ def keygen_rate(xb, torch, dev, sh, sets=((0x02, 8), (0x03, 1))):
 
     run()  # warm-up (scratch growth)
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    run()
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    times = []
+    for _ in range(max(1, repeats)):
+        for *_, d_pk, _d_sk in jobs:
+            d_pk.fill_(0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = float(np.median(times))
+    # byte check of every public key against the golden keys of the same seeds
+    correct = None
+    if os.path.exists(KEYGEN_GOLDEN):
+        gold = {(g["oid"], g["seed"]): g["pk"] for g in json.load(open(KEYGEN_GOLDEN))["keys"]}
+        correct = True
+        checked = 0
+        for (oid, seeds_np), (_, count, p, _s, d_pk, _k) in zip(keygen_seeds(sets), jobs):
+            got = d_pk.cpu().numpy().reshape(count, 2 * p.n)
+            for i in range(count):
+                want = gold.get((oid, seeds_np[i].tobytes().hex()))
+                if want is None:
+                    correct = None if checked == 0 else correct
+                    continue
+                checked += 1
+                correct = correct and got[i].tobytes().hex() == want
+        if checked == 0:
+            correct = None
     leaves = sum(count << p.full_height for _, count, p, *_ in jobs)
     leaf_compr = 67 * 2 + 67 * 15 * 4 + 66 * 6  # PRF_keygen, 15 F per chain, L-tree
     comp = sum(count * ((leaf_compr << p.full_height) + 6 * ((1 << p.full_height) - 1)) for _, count, p, *_ in jobs)
     what = " + ".join(f"{count} x XMSS-SHA2_{p.full_height}_256" for _, count, p, *_ in jobs)
     return {"metric": f"keygen leaves/s: {what} ({leaves:,} leaves)",
-            "value": leaves / (ms / 1e3), "unit": "leaves/s", "ms": ms, "gcompr_s": comp / (ms / 1e3) / 1e9,
-            "compressions": comp}
+            "value": leaves / (ms / 1e3), "unit": "leaves/s", "ms": ms, "ms_runs": times,
+            "gcompr_s": comp / (ms / 1e3) / 1e9, "compressions": comp, "correct": correct,
+            "check": "every public key equal to tests/golden/keygen_config3.json (same seeds; made by the "
+                     "reference C path for h=16 and the threaded oracle for h=20)"}
 
 
 def run_keygen(args):
@@ -609,81 +726,80 @@ def cpu_baseline(w, budget_s: float = 2.5, sample=None, pool=None):
 
 
 def run_reference(args, rank: int, world: int):
+    """The reference arm: the reference's own CPU verify (xmss_sign_open of
+    the reference C path compiled into oracle/_ref, cuxmss/xmss.c:45-60) on
+    every host core, one spawned process per core, over the same 4,096
+    signed messages as the GPU arm (built byte for byte by the CPU oracle,
+    so no GPU code runs in this arm).  A step verifies all of them once."""
     if rank != 0:
         return None
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    w = None
-    try:
-        import xmss_b200 as xb
-
-        xb.init(0)
-        w = make_workload(xb, 0)
-    except Exception as ex:  # no GPU: build the sample with the CPU oracle
-        log(f"workload via the CPU oracle ({ex})")
-        w = make_workload_cpu()
     import multiprocessing as mp
 
-    rng = np.random.default_rng(SEED + 99)
-    sample = rng.choice(len(w["sms"]), min(512, len(w["sms"])), replace=False)
-    sms = [w["sms"][i] for i in sample]
-    pks = [bytes(w["pks"][w["keyix"][i]]) for i in sample]
+    t0 = time.perf_counter()
+    w = make_workload_cpu(0)
+    log(f"reference arm: workload built on the host in {time.perf_counter() - t0:.1f} s")
+    sms = w["sms"]
+    pks = [bytes(w["pks"][w["keyix"][i]]) for i in range(len(sms))]
+    expect = [int(x) for x in w["expect"]]
     cores = os.cpu_count() or 1
-    vals = []
+    chunk = (len(sms) + cores - 1) // cores
+    ranges = [(a, min(a + chunk, len(sms))) for a in range(0, len(sms), chunk)]
+    times, ok = [], True
     with mp.get_context("spawn").Pool(cores, initializer=_cpu_init, initargs=(sms, pks)) as pool:
-        for _ in range(args.warmup):
-            cpu_baseline(w, budget_s=0.0, sample=sample, pool=pool)
-        for _ in range(args.steps):
-            vals.append(cpu_baseline(w, budget_s=0.0, sample=sample, pool=pool))
-    value = float(np.mean([v["value"] for v in vals]))
-    cores = vals[0]["cores"]
+        for i in range(args.warmup + args.steps):
+            s0 = time.perf_counter()
+            res = [r for part in pool.map(_cpu_verify_range, ranges) for r in part]
+            dt = time.perf_counter() - s0
+            ok = ok and res == expect
+            if i >= args.warmup:
+                times.append(dt)
+    kind = _cpu_verifier()[1]
+    total = float(sum(times))
+    value = len(sms) * len(times) / total
     return {
-        "metric": "XMSS-SHA2_10_256 batched verifies/s (4096 sigs, 64 keys, mlen 32B-4KB log-uniform, 10% bit-flipped)",
-        "value": value, "unit": "verifies/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * len(sample) / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u32", "data": "synthetic (seeded)", "impl": "reference",
-        "config": {"workload": "batched verify, XMSS-SHA2_10_256", "oid": OID, "signatures": NUM_SIGS,
-                   "keys": NUM_KEYS, "mlen": "log-uniform 32..4096 B", "bitflip_fraction": 0.1,
-                   "parallelism": "host threads"},
-        "correct": all(v["correct"] for v in vals),
-        "cpu_baseline": {"value": value, "unit": "verifies/s", "cores": cores, "kind": vals[0]["kind"],
-                         "sample": f"each step verifies the same 512-signature sample of the workload on {cores} threads"},
+        "metric": METRIC, "value": value, "unit": "verifies/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded keys and messages; the same signed messages as the GPU arm, made by the CPU "
+                "oracle; accept bitmap checked)",
+        "impl": "reference",
+        "config": workload_config(w, world),
+        "correct": ok,
+        "cpu_baseline": {"value": value, "unit": "verifies/s", "cores": cores, "kind": kind,
+                         "sample": f"each step verifies the whole {len(sms)}-signature workload once on {cores} "
+                                   "processes (reference xmss_sign_open from oracle/_ref)"},
         "e2e": {"value": value, "unit": "verifies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-
-
-def make_workload_cpu(count: int = 512, keys: int = 8):
-    """A sample of the same workload shape built with the CPU oracle (no-GPU
-    hosts only; fewer keys so the trees build in seconds)."""
-    from oracle import Oracle
-
-    o = Oracle()
-    rng = np.random.default_rng(SEED)
-    p = o.params(OID)
-    seeds = [rng.bytes(3 * p.n) for _ in range(keys)]
-    keyix = rng.integers(0, keys, count).astype(np.uint32)
-    idx = rng.integers(0, 1 << p.full_height, count)
-    mlen = np.exp(rng.uniform(np.log(32), np.log(4096), count)).astype(np.int64)
-    trees, pks = [], np.zeros((keys, 4 + 2 * p.n), np.uint8)
-    for k, s in enumerate(seeds):
-        trees.append(o.tree_nodes(p, s[:32], s[64:], 0, 0, os.cpu_count()))
-        pks[k] = np.frombuffer(b"\0\0\0\x01" + trees[k][-32:] + s[64:], np.uint8)
-    sms, expect = [], np.zeros(count, np.int32)
-    for i in range(count):
-        k = int(keyix[i])
-        s = seeds[k]
-        sk = int(idx[i]).to_bytes(4, "big") + s[:64] + trees[k][-32:] + s[64:]
-        sm = bytearray(o.sign(p, sk, rng.bytes(int(mlen[i])), trees=trees[k])[2])
-        if i % 10 == 0:
-            sm[int(rng.integers(0, len(sm)))] ^= 1 << int(rng.integers(0, 8))
-            expect[i] = -1
-        sms.append(bytes(sm))
-    return dict(p=p, pks=pks, keyix=keyix, sms=sms, expect=expect, mean_mlen=float(mlen.mean()))
 
 
 # ---------------------------------------------------------------------------
 
 MIX_SETS = (("XMSSMT-SHA2_20/2_256", 0x01, True), ("XMSSMT-SHA2_40/4_256", 0x04, True),
             ("XMSS-SHA2_10_512", 0x04, False), ("XMSS-SHAKE_10_256", 0x07, False))
+MIX_COUNT = 2048
+MIX_GOLDEN = os.path.join(ROOT, "tests", "golden", "mix_config4.json")
+
+
+def mix_draws(rng, n: int, full_height: int, count: int = MIX_COUNT):
+    """Seeded inputs of one parameter set of the XMSS^MT / wide-hash mix:
+    key seeds, the first index, the index cap per key and the messages
+    (log-uniform in 32 B..64 KB).  Signatures run at consecutive indices;
+    a key of height 10 has 1,023 usable ones, so such sets take two keys.
+    Signature i uses key i // cap at index start + i % cap."""
+    cap = min((1 << full_height) - 1, count)
+    nkeys = -(-count // cap)
+    seeds = np.frombuffer(rng.bytes(nkeys * 3 * n), np.uint8).reshape(nkeys, -1).copy()
+    start = 0 if cap < count else int(rng.integers(0, (1 << min(full_height, 40)) - count))
+    mlen = np.exp(rng.uniform(np.log(32), np.log(65536), count)).astype(np.int64)
+    msgs = [rng.bytes(int(L)) for L in mlen]
+    return seeds, start, cap, msgs
+
+
+def mix_all_draws(params_of):
+    """mix_draws of every set in MIX_SETS from one seeded stream, in order;
+    params_of(oid, mt) -> (n, full_height)."""
+    rng = np.random.default_rng(SEED + 4)
+    return [mix_draws(rng, *params_of(oid, mt)) for _, oid, mt in MIX_SETS]
 
 
 def run_mix(args):
@@ -697,6 +813,14 @@ def run_mix(args):
     xb.init(0)
     dev = torch.device("cuda", 0)
     sh = torch.cuda.current_stream(dev).cuda_stream
+    return mix_rates(xb, torch, dev, sh)
+
+
+def mix_rates(xb, torch, dev, sh):
+    """Signs/s and verifies/s of the four mix sets, each set's chain kernels
+    against the compression rate of its own hash core, and a byte check of
+    every signature against the golden digests (tests/golden/mix_config4.json,
+    made by the oracle from the same seeds)."""
     # compression-rate probes of the three cores (same code as the kernels)
     probe_blocks = 148 * 16 * 4
     sink = torch.zeros(probe_blocks * 128, dtype=torch.int32, device=dev)
@@ -709,20 +833,16 @@ def run_mix(args):
         e1.record()
         torch.cuda.synchronize()
         probe[kind] = probe_blocks * 128 * iters / (e0.elapsed_time(e1) / 1e3) / 1e9
-    rng = np.random.default_rng(SEED + 4)
     out = {"workload": "mix", "sets": [],
            "probe_g_per_s": {"sha256": max(probe[10], probe[11]), "sha512": probe[2], "keccak_f1600": probe[1]}}
-    for name, oid, mt in MIX_SETS:
+    gold = {g["set"]: g for g in json.load(open(MIX_GOLDEN))["sets"]} if os.path.exists(MIX_GOLDEN) else {}
+    draws = mix_all_draws(lambda oid, mt: (xb.parse_oid(oid, mt).n, xb.parse_oid(oid, mt).full_height))
+    for (name, oid, mt), (seeds, start, cap, msgs) in zip(MIX_SETS, draws):
         p = xb.parse_oid(oid, mt)
-        count = 2048
-        # consecutive indices per key; a key of height 10 has 1,023 usable ones
-        cap = min((1 << p.full_height) - 1, count)
-        nkeys = -(-count // cap)
-        seeds = np.frombuffer(rng.bytes(nkeys * 3 * p.n), np.uint8).reshape(nkeys, -1)
+        count = len(msgs)
+        mlen = np.array([len(m) for m in msgs])
+        nkeys = seeds.shape[0]
         pks, sks = xb.keypair_batch(oid, mt, seeds)
-        start = 0 if cap < count else int(rng.integers(0, (1 << min(p.full_height, 40)) - count))
-        mlen = np.exp(rng.uniform(np.log(32), np.log(65536), count)).astype(np.int64)
-        msgs = [rng.bytes(int(L)) for L in mlen]
         kix = (np.arange(count) // cap).astype(np.uint32)
         rows = np.array(sks[kix])
         for i in range(count):
@@ -756,14 +876,23 @@ def run_mix(args):
         achieved = w.f_calls * per_f / (chains_ms / 1e3) / 1e9
         roof = {"core": core, "achieved_g_per_s": achieved, "peak_g_per_s": out["probe_g_per_s"][core],
                 "frac": achieved / out["probe_g_per_s"][core], "chains_ms": chains_ms}
-        out["sets"].append({"set": name, "keys": nkeys, "signs": count, "signs_per_s": count / t_sign,
-                            "chain_roofline": roof,
+        # byte check: sha256 over every signed message in order, and the
+        # public keys, against the oracle's digests of the same seeds
+        import hashlib
+
+        digest = hashlib.sha256(b"".join(sms)).hexdigest()
+        g = gold.get(name)
+        byte_exact = None if g is None else (digest == g["sms_sha256"] and
+                                             [pk[4:].tobytes().hex() for pk in pks] == g["pks"])
+        out["sets"].append({"set": name, "keys": nkeys, "signs": count, "first_index": start,
+                            "signs_per_s": count / t_sign, "chain_roofline": roof,
                             "verifies_per_s": count / t_ver, "sign_s": t_sign, "verify_s": t_ver,
                             "mean_mlen": float(mlen.mean()), "all_signed": bool((ret == 0).all()),
-                            "all_verified": bool((st == 0).all()),
+                            "all_verified": bool((st == 0).all()), "byte_exact_vs_oracle": byte_exact,
                             "verify_work": {"hmsg_blocks": w.hmsg_blocks, "f_calls": w.f_calls,
                                             "h_calls": w.h_calls}})
         log(out["sets"][-1])
+    out["correct"] = all(s["all_signed"] and s["all_verified"] and s["byte_exact_vs_oracle"] for s in out["sets"])
     return out
 
 
@@ -846,6 +975,54 @@ def _serve_trace(xb, rng, n, rate, keys, kids, pool, rand):
     tr["smlen_ptr"] = np.where(sign, u64(smlen.ctypes.data) + u64(8) * np.arange(n, dtype=u64), u64(0))
     tr["pk_ptr"] = np.where(sign, u64(0), u64(pool["pk"].ctypes.data) + u64(pool["pk_stride"]) * k.astype(u64))
     return tr, (out, smlen, sign, k, out_off, mlen, moff)
+
+
+def _serve_oracle_check(keys, used_idx, keep, rand, per_set: int = 2):
+    """Byte check of served signatures against the CPU oracle: per parameter
+    set, up to `per_set` sign requests of one key are signed again by the
+    oracle (xmss_core.c:183-273) with the one-time index the server issued,
+    and must be identical byte for byte.  The oracle builds each subtree on
+    all host cores; for the height-16 set (about a minute per subtree there)
+    the oracle's verify (xmss_commons.c:136-215) accepts the signature and
+    its index bytes are checked instead."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+
+    o = Oracle()
+    cores = os.cpu_count() or 1
+    out, smlen, sign, k, out_off, mlen, moff = keep
+    res = {"ok": True, "signed_again": 0, "opened": 0}
+    trees = {}
+    for si in range(len(SERVE_SETS)):
+        reqs = [int(i) for i in np.flatnonzero(sign) if keys[int(k[i])][0] == si]
+        if not reqs:
+            continue
+        key0 = int(k[reqs[0]])
+        for i in [r for r in reqs if int(k[r]) == key0][:per_set]:
+            _, mt, p, pk, sk = keys[key0]
+            po = o.params(int.from_bytes(sk[:4], "big"), mt)
+            ib, n, th = po.index_bytes, po.n, po.tree_height
+            sm = out[int(out_off[i]):int(out_off[i]) + int(smlen[i])].tobytes()
+            m = rand[int(moff[i]):int(moff[i]) + int(mlen[i])].tobytes()
+            index = int(used_idx[i])
+            skx = index.to_bytes(ib, "big") + sk[4 + ib:]
+            if th > 10:
+                good = o.sign_open(po, sm, pk[4:])[0] == 0 and sm[:ib] == skx[:ib]
+                res["opened"] += 1
+            else:
+                layers = []
+                for layer in range(po.d):
+                    tree = index >> (th * (layer + 1)) if th * (layer + 1) < 64 else 0
+                    if (layer, tree) not in trees:
+                        trees[(layer, tree)] = o.tree_nodes(po, skx[ib:ib + n], skx[ib + 3 * n:ib + 4 * n], layer,
+                                                            tree, cores)
+                    layers.append(trees[(layer, tree)])
+                r, _, smo = o.sign(po, skx, m, trees=b"".join(layers))
+                good = r == 0 and smo == sm
+                res["signed_again"] += 1
+            res["ok"] = res["ok"] and bool(good)
+        trees.clear()
+    return res
 
 
 def _plain_per_call(xb, keys, pool_sms, rng, rand, n):
@@ -931,6 +1108,7 @@ def run_serve(args):
 
     rates = [float(r) for r in args.serve_rates.split(",")]
     sweep = []
+    oracle_check = None
     for rate in rates + [0.0]:
         n = args.serve_n if rate == 0 else int(min(args.serve_n, max(2000, rate * args.serve_seconds)))
         tr, keep = _serve_trace(xb, rng, n, rate, keys, kids, pool, rand)
@@ -939,18 +1117,10 @@ def run_serve(args):
         bt = [b for b in srv.batch_trace() if b["seq"] > seq0]
         out, smlen, sign, k, out_off, mlen, moff = keep
         ok = bool((ret == 0).all())
-        # spot-check: signatures byte-for-byte verified by the batch API
-        chk = np.flatnonzero(sign)[:64]
-        for si in range(len(SERVE_SETS)):
-            sel = [i for i in chk if keys[int(k[i])][0] == si]
-            if not sel:
-                continue
-            mt = keys[int(k[sel[0]])][1]
-            sms = [out[int(out_off[i]):int(out_off[i]) + int(smlen[i])].tobytes() for i in sel]
-            b2, o2, l2 = xb.pack(sms, align=16)
-            pks = np.stack([np.frombuffer(keys[int(k[i])][3], np.uint8) for i in sel])
-            st = xb.sign_open_batch(mt, b2, o2, l2, pks, np.arange(len(sel), dtype=np.uint32))
-            ok &= bool((st == 0).all())
+        if rate == 0 and args.serve_check:
+            # the burst: a sample of its signatures signed again by the oracle
+            oracle_check = _serve_oracle_check(keys, idx, keep, rand, per_set=args.serve_check)
+            ok &= oracle_check["ok"]
         lat_ms = lat / 1e3
         row = {"offered_per_s": rate if rate else "burst", "requests": n, "elapsed_s": el,
                "achieved_per_s": n / el, "all_ok": ok,
@@ -982,8 +1152,11 @@ def run_serve(args):
         "offered_per_s"] and r["p99_sign_ms"] <= 10.0]
     best = max((r["achieved_per_s"] for r in sustained), default=None)
     burst = sweep[-1]["achieved_per_s"]
+    met = [r["offered_per_s"] for r in sweep if r["offered_per_s"] != "burst" and r["p99_sign_ms"] <= 10.0]
     return {"workload": "serve", "metric": "served requests/s (30% sign / 70% verify, 256 resident keys)",
             "unit": "requests/s", "value": burst, "sustained_p99_sign_le_10ms_per_s": best,
+            "highest_offered_rate_with_p99_sign_le_10ms": max(met, default=None),
+            "correct": all(r["all_ok"] for r in sweep), "oracle_check": oracle_check,
             "vs_plain_per_call": burst / plain["requests_per_s"], "plain_per_call": plain, "sweep": sweep,
             "server": {"max_batch": args.serve_batch, "slots": args.serve_slots, "stats": stats},
             "config": {"workload": "serve", "keys": len(keys), "sets": [s for s, _ in SERVE_SETS],
@@ -1007,7 +1180,13 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--serve-plain-n", type=int, default=150, help="requests of the per-call comparison")
     ap.add_argument("--keygen-small", action="store_true", help="keygen workload: one h=16 key (profiling)")
+    ap.add_argument("--serve-check", type=int, default=2,
+                    help="burst signatures per parameter set signed again by the oracle (0: none)")
+    ap.add_argument("--sec-serve-rates", default="10000,30000,100000",
+                    help="offered rates of the short serving sweep in the default line")
     ap.add_argument("--skip-keygen", action="store_true")
+    ap.add_argument("--skip-mix", action="store_true")
+    ap.add_argument("--skip-serve", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=2.5)
     args = ap.parse_args()

@@ -16,6 +16,7 @@
 
 #include "../../include/params.h"
 #include "../../include/randombytes.h"
+#include "../../include/utils.h"
 #include "../../include/xmss.h"
 #include "../../include/xmss_b200.h"
 #include "../../include/xmss_core.h"
@@ -310,6 +311,20 @@ extern "C" __attribute__((weak)) void randombytes(unsigned char* x, unsigned lon
 }
 
 // ===========================================================================
+// utils.h
+// ===========================================================================
+
+extern "C" void ull_to_bytes(unsigned char* out, unsigned int outlen, unsigned long long in)
+{
+    be_write(out, outlen, in);
+}
+
+extern "C" unsigned long long bytes_to_ull(const unsigned char* in, unsigned int inlen)
+{
+    return be_read(in, inlen);
+}
+
+// ===========================================================================
 // xmss_core.h
 // ===========================================================================
 
@@ -596,6 +611,14 @@ extern "C" int xmss_b200_sign_open_device_persistent(uint32_t oid, int mt, uint3
         e.begin(st);
         e.verify_persistent(ops, p, count, d_sm, d_sm_off, d_smlen, d_pk, npk, d_pk_index, d_status, st);
         e.end(st);
+        return kOk;
+    });
+}
+
+extern "C" int xmss_b200_set_wait_bound(unsigned long long ns)
+{
+    return guarded([&](Engine& e) {
+        e.persist_wait_ns = ns ? ns : Engine::kDefaultWaitNs;
         return kOk;
     });
 }

@@ -391,6 +391,7 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
     v.key = d_pk_index;
     v.key_root = d_pk;
     v.key_stride = 2 * n;
+    v.npk = npk;
     v.node = w.node.as<uint8_t>((size_t)count * n);
     v.lens = w.lens.as<uint8_t>((size_t)count * len);
     v.idx = w.idx.as<uint64_t>(count);
@@ -472,6 +473,7 @@ void Engine::verify_persistent(const FamilyOps* ops, const xmss_params& p, uint3
     v.key = d_pk_index;
     v.key_root = d_pk;
     v.key_stride = 2 * n;
+    v.npk = npk;
     v.node = w.node.as<uint8_t>((size_t)count * n);
     v.lens = w.lens.as<uint8_t>((size_t)count * len);
     v.idx = w.idx.as<uint64_t>(count);
@@ -504,6 +506,7 @@ void Engine::verify_persistent(const FamilyOps* ops, const xmss_params& p, uint3
     q.ctx = w.ctx.get((size_t)npk * ops->ctx_bytes);
     q.npk = npk;
     q.groups = groups;
+    q.wait_ns = persist_wait_ns;
     XB_CUDA(cudaMemsetAsync(st8, 0, 8 + words * 4, st));
     ops->verify_persist(v, q, st);
     XB_CUDA(cudaGetLastError());

@@ -207,6 +207,12 @@ class Engine {
     // Batches of at least Tuning::split_min signatures are verified as two
     // groups split at Tuning::short_hmsg_blocks hash blocks of H_msg.
 
+    // Bound of one dependency wait inside a persistent launch, in ns of the
+    // GPU's global timer (xmss_b200_set_wait_bound).  A wait that runs out
+    // ends the launch with -3 for every item instead of waiting on.
+    static constexpr unsigned long long kDefaultWaitNs = 8000000000ull;
+    unsigned long long persist_wait_ns = kDefaultWaitNs;
+
     // Work counters of the last verify (see xmss_b200_last_verify_work).
     void last_verify_work(unsigned long long out[3]);
 

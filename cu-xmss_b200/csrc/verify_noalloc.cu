@@ -23,9 +23,14 @@
 //     wrong results; callers serialise them.  The array keeps whatever the
 //     last call left in it; every buffer that must start at zero is cleared
 //     on the stream at the start of each call.
-//   * The first call on each device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before capturing any stream.
+//   * The first call on each device is its set-up: with that device current
+//     it looks up the array's device address (cudaGetSymbolAddress), which
+//     loads the library's device code on that device if it is not loaded
+//     yet; make that first call before capturing any stream.  Later calls
+//     repeat the lookup (a table lookup once the code is loaded, no
+//     allocation), so the address is never stale: after cudaDeviceReset, or
+//     under another context, the call uses the array of the context that is
+//     current then.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -44,27 +49,19 @@ void set_last_error(const std::string& msg);  // api.cu
 namespace {
 
 constexpr size_t kNoallocScratchBytes = 8u << 20;
-constexpr int kMaxDevices = 64;
 
 // The fixed scratch array.  In host code this name is only a stand-in for the
 // symbol; kernels receive the device address looked up below.
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoallocScratchBytes];
 
-std::mutex g_addr_mu;
-void* g_addr[kMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on `dev` (which must be current).
-cudaError_t scratch_address(int dev, void** out)
+// Device address of g_noalloc_scratch in the current context (the device the
+// call runs on must be current).
+cudaError_t scratch_address(void** out)
 {
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> g(g_addr_mu);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_addr[dev] = p;
-    }
-    *out = g_addr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    *out = p;
     return cudaSuccess;
 }
 
@@ -118,10 +115,8 @@ extern "C" int xmss_b200_sign_open_device_noalloc(uint32_t oid, int mt, uint32_t
                        std::to_string(kNoallocScratchBytes) + "; split the batch");
         return -1;
     }
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
     uint8_t* base = nullptr;
-    if (e == cudaSuccess) e = scratch_address(dev, (void**)&base);
+    cudaError_t e = scratch_address((void**)&base);
     if (e != cudaSuccess) {
         set_last_error(std::string("xmss_b200_sign_open_device_noalloc: ") + cudaGetErrorString(e));
         return -3;
@@ -135,6 +130,7 @@ extern "C" int xmss_b200_sign_open_device_noalloc(uint32_t oid, int mt, uint32_t
     v.key = d_pk_index;
     v.key_root = d_pk;
     v.key_stride = 2 * n;
+    v.npk = npk;
     v.node = base + o_node;
     v.lens = base + o_lens;
     v.idx = (uint64_t*)(base + o_idx);

@@ -24,9 +24,10 @@
 // and a ticket is only taken by a running warp, the smallest unfinished
 // ticket never waits: the launch always completes, whatever the residency
 // of its CTAs.  No CTA-wide barrier is used inside the loop.  Each wait is
-// still bounded (kPersistWaitNs of the global timer); one that runs out
-// sets an error flag, every warp then leaves the loop, and the last CTA to
-// exit writes -3 into every status.
+// still bounded (PersistArgs::wait_ns of the global timer, 8 s unless the
+// caller sets another bound); one that runs out sets an error flag, every
+// warp then leaves the loop, and the last CTA to exit writes -3 into every
+// status.
 //
 // Results are those of the multi-launch pipeline (same per-node hash calls;
 // only the schedule differs).
@@ -47,13 +48,14 @@ struct PersistArgs {
     uint32_t* hpre_done;         // [G] h_pre tasks finished
     uint32_t* list;              // [G][32*LEN] chain items (s*LEN + chain) of the group's current layer
     void* ctx;                   // [npk] F::Ctx, written by the ctx tasks
+    unsigned long long wait_ns;  // bound of one dependency wait (%globaltimer ns)
     uint32_t npk;
     uint32_t groups;
 };
 
-// Bound of a single dependency wait (ns of %globaltimer).  Inputs of a task
-// are produced by tasks already running, so a legitimate wait lasts at most
-// about one H_msg: 8 s is a message of several hundred MB.
+// Default bound of a single dependency wait (ns of %globaltimer).  Inputs of
+// a task are produced by tasks already running, so a legitimate wait lasts at
+// most about one H_msg: 8 s is a message of several hundred MB.
 constexpr unsigned long long kPersistWaitNs = 8000000000ull;
 
 // L-tree shape (xmss_commons.c:16-49): level l reduces cnt(l) nodes into
@@ -117,7 +119,8 @@ __device__ __forceinline__ unsigned long long global_ns()
 // wait ran out (the error flag is then set) or another warp failed.  Polls
 // are relaxed loads followed by one acquire fence, so a waiting warp does not
 // order its SM's L1 against the GPU on every poll.
-__device__ __forceinline__ bool persist_wait(const uint32_t* c, uint32_t target, uint32_t* err)
+__device__ __forceinline__ bool persist_wait(const uint32_t* c, uint32_t target, uint32_t* err,
+                                             unsigned long long bound_ns)
 {
     bool ok = true;
     if (ld_acquire(c) < target) {
@@ -128,7 +131,7 @@ __device__ __forceinline__ bool persist_wait(const uint32_t* c, uint32_t target,
                 ok = false;
                 break;
             }
-            if (global_ns() - t0 > kPersistWaitNs) {
+            if (global_ns() - t0 > bound_ns) {
                 atomicExch(err, 1u);
                 ok = false;
                 break;
@@ -260,7 +263,7 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
             bool live = false;
             if (s < v.count) {
                 const uint64_t smlen = v.smlen[s];
-                if (smlen < v.sig_bytes) {  // the reference would underflow here; reject
+                if (!verify_input_ok(v, s)) {  // too short, or a key index outside the table
                     v.status[s] = -1;
                 } else {
                     const uint8_t* sm = v.sm + v.sm_off[s];
@@ -287,7 +290,7 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
         if (t < n_hpre) {  // -------- h_pre of one H node of one layer, for a group
             const uint32_t g = (uint32_t)(t / ((unsigned long long)d * nh));
             const uint32_t k = (uint32_t)(t - (unsigned long long)g * d * nh);
-            if (!persist_wait(&q.hdr[2], (uint32_t)K, err)) break;
+            if (!persist_wait(&q.hdr[2], (uint32_t)K, err, q.wait_ns)) break;
             const uint32_t s = g * 32 + lane;
             if (s < v.count) verify_hpre_item<F>(v, ctx, (uint64_t)s * d * nh + k);
             persist_signal(&q.hpre_done[g]);
@@ -301,8 +304,8 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
         if (r < (unsigned long long)G * LEN) {  // -------- 32 chains of a group's list
             const uint32_t c = (uint32_t)(r / G), g = (uint32_t)(r - (unsigned long long)c * G);
             const uint32_t gl = g * d + layer;
-            if (!persist_wait(&q.ready[gl], 1u, err)) break;
-            if (layer == 0 && !persist_wait(&q.hdr[2], (uint32_t)K, err)) break;
+            if (!persist_wait(&q.ready[gl], 1u, err, q.wait_ns)) break;
+            if (layer == 0 && !persist_wait(&q.hdr[2], (uint32_t)K, err, q.wait_ns)) break;
             const uint32_t e = c * 32 + lane;
             if (e < q.ntot[gl]) {
                 const uint32_t item = q.list[(uint64_t)g * 32 * LEN + e];
@@ -336,9 +339,9 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
             const uint32_t g = (uint32_t)(r / items), p = (uint32_t)(r - (unsigned long long)g * items);
             const uint32_t gl = g * d + layer;
             if (lev == 0) {
-                if (!persist_wait(&q.chains_done[gl], (uint32_t)LEN, err)) break;
-                if (!persist_wait(&q.hpre_done[g], d * nh, err)) break;
-            } else if (!persist_wait(&q.lt_done[gl * 8 + lev - 1], (uint32_t)lt_items(LEN, lev - 1), err)) {
+                if (!persist_wait(&q.chains_done[gl], (uint32_t)LEN, err, q.wait_ns)) break;
+                if (!persist_wait(&q.hpre_done[g], d * nh, err, q.wait_ns)) break;
+            } else if (!persist_wait(&q.lt_done[gl * 8 + lev - 1], (uint32_t)lt_items(LEN, lev - 1), err, q.wait_ns)) {
                 break;
             }
             const uint32_t s = g * 32 + lane;
@@ -368,7 +371,7 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
         r -= (unsigned long long)G * LT;
         {  // -------- compute_root of a group, then the next layer's list or the verdict
             const uint32_t g = (uint32_t)r, gl = g * d + layer;
-            if (!persist_wait(&q.lt_done[gl * 8 + LV - 1], 1u, err)) break;
+            if (!persist_wait(&q.lt_done[gl * 8 + LV - 1], 1u, err, q.wait_ns)) break;
             const uint32_t s = g * 32 + lane;
             const bool live = s < v.count && v.status[s] == 0;
             bool next_live = false;

@@ -237,9 +237,10 @@ struct VerifyArgs {
     const uint8_t* sm;        // concatenated signed messages
     const uint64_t* sm_off;   // [count] byte offset of each sm
     const uint64_t* smlen;    // [count]
-    const uint32_t* key;      // [count] key index
+    const uint32_t* key;      // [count] key index, checked against npk on the device
     const uint8_t* key_root;  // public root of key k at key_root + k * key_stride
     uint32_t key_stride;
+    uint32_t npk;             // keys at key_root; a signature naming key >= npk is rejected (-1)
     uint8_t* node;            // [count][N] running message / root
     uint8_t* lens;            // [count][LEN] chain start positions
     uint64_t* idx;            // [count]
@@ -293,6 +294,15 @@ __device__ __forceinline__ void flush_hist(uint32_t* sh_hist, uint32_t* hist)
 
 // Signatures handled by this launch sequence: all of them, or the selection.
 __device__ __forceinline__ uint32_t sel_count(const VerifyArgs& v) { return v.sel ? *v.sel_n : v.count; }
+
+// Inputs a signature must have before anything of it is read: a signed
+// message at least sig_bytes long (the reference would underflow its message
+// length there, xmss_commons.c:158) and a key index inside the key table.
+// Failing either rejects the signature (-1); every later step skips it.
+__device__ __forceinline__ bool verify_input_ok(const VerifyArgs& v, uint32_t s)
+{
+    return v.smlen[s] >= v.sig_bytes && v.key[s] < v.npk;
+}
 __device__ __forceinline__ uint32_t sel_sig(const VerifyArgs& v, uint32_t i) { return v.sel ? v.sel[i] : i; }
 
 template <class F>
@@ -334,7 +344,7 @@ __device__ __forceinline__ void verify_hpre_item(const VerifyArgs& v, const type
     const uint64_t item = (uint64_t)s * v.d * nh + rem;
     const uint32_t layer = rem / nh;
     uint32_t node = rem - layer * nh;
-    if (v.smlen[s] < v.sig_bytes) return;
+    if (!verify_input_ok(v, s)) return;
     const uint64_t idx = bytes_be(v.sm + v.sm_off[s], (int)v.index_bytes);
     uint32_t leaf;
     uint64_t tree;
@@ -372,7 +382,7 @@ __global__ void __launch_bounds__(64) k_verify_prep(VerifyArgs v, uint32_t hmsg_
         if (i < sel_count(v)) {
             const uint32_t s = sel_sig(v, i);
             const uint64_t smlen = v.smlen[s];
-            if (smlen < v.sig_bytes) {  // the reference would underflow here; reject
+            if (!verify_input_ok(v, s)) {
                 v.status[s] = -1;
             } else {
                 const uint8_t* sm = v.sm + v.sm_off[s];

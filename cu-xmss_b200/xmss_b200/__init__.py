@@ -136,6 +136,7 @@ lib.xmss_b200_core_hash_batch.argtypes = [C.c_uint, C.c_uint, C.c_uint32, _u8p, 
 lib.xmss_b200_last_verify_work.argtypes = [C.POINTER(Work)]
 lib.xmss_b200_sign_open_device_noalloc.argtypes = lib.xmss_b200_sign_open_device.argtypes
 lib.xmss_b200_sign_open_device_persistent.argtypes = lib.xmss_b200_sign_open_device.argtypes
+lib.xmss_b200_set_wait_bound.argtypes = [C.c_ulonglong]
 lib.xmss_b200_profile.argtypes = [C.c_int]
 lib.xmss_b200_phase_ms.argtypes = [C.POINTER(C.c_double)]
 lib.xmss_b200_rate_probe.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
@@ -553,6 +554,14 @@ def sign_open_device_persistent(oid: int, mt: bool, count: int, d_sm: int, d_sm_
                                                          d_pk_index, d_status, stream), "sign_open_device_persistent")
     if r:
         raise ValueError(f"sign_open_device_persistent returned {r}: {last_error()}")
+
+
+def set_wait_bound(ns: int) -> None:
+    """xmss_b200_set_wait_bound: bound of one dependency wait inside later
+    persistent launches, in ns (0 = the default of 8 s)."""
+    r = _check(lib.xmss_b200_set_wait_bound(int(ns)), "set_wait_bound")
+    if r:
+        raise ValueError(f"set_wait_bound returned {r}: {last_error()}")
 
 
 def sign_open_device_noalloc(oid: int, mt: bool, count: int, d_sm: int, d_sm_off: int, d_smlen: int, d_pk: int,

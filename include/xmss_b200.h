@@ -83,6 +83,14 @@ int xmss_b200_sign_open_device_persistent(uint32_t oid, int mt, uint32_t count, 
                                           const uint8_t *d_pk, uint32_t npk, const uint32_t *d_pk_index,
                                           int *d_status, void *stream);
 
+/* Bound of one dependency wait inside a persistent launch, in ns of the
+ * GPU's global timer;
+ * 0 restores the default of 8 s.  A wait that runs out ends the launch with
+ * -3 in every status instead of waiting on; the bound is passed to each
+ * launch as an argument, so it applies to launches made after the call.
+ * No reference counterpart (the reference has no persistent launch). */
+int xmss_b200_set_wait_bound(unsigned long long ns);
+
 /* Pipelined form of xmss_b200_sign_open_batch: enqueues the copy of the
  * signed messages from the caller's memory, the verify, and the copy of the
  * statuses into `status` on `stream` (cudaStream_t as void*) and returns.
