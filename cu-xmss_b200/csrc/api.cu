@@ -690,7 +690,7 @@ extern "C" int xmss_b200_phase_ms(double ms[5])
 
 extern "C" int xmss_b200_rate_probe(int kind, uint32_t blocks, uint32_t iters, uint32_t* d_sink, void* stream)
 {
-    if ((kind != 0 && kind != 1 && kind != 2 && (kind < 10 || kind > 13) && kind != 20 && kind != 21 && kind != 23) || !blocks ||
+    if ((kind != 0 && kind != 1 && kind != 2 && (kind < 10 || kind > 19) && kind != 20 && kind != 21 && kind != 23) || !blocks ||
         !d_sink)
         return kBad;
     return guarded([&](Engine& e) {

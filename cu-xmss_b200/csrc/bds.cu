@@ -110,7 +110,8 @@ class Subtrees {
         xb::TreeJob* dj = djobs_.as<xb::TreeJob>(batch);
         XB_CUDA(cudaMemcpyAsync(dj, jobs.data(), batch * sizeof(xb::TreeJob), cudaMemcpyHostToDevice, st));
         uint8_t* dn = dnodes_.as<uint8_t>(batch * tree_bytes_);
-        e_.build_trees(ops_, dj, (uint32_t)batch, (int)p_.tree_height, dn, ctx_.get(1), st, w_);
+        e_.build_trees(ops_, dj, (uint32_t)batch, (int)p_.tree_height, dn, ctx_.get(1), st, w_,
+                       xb::Engine::subtree_k(p_, (uint32_t)batch));
         std::vector<uint8_t> all(batch * tree_bytes_);
         XB_CUDA(cudaMemcpyAsync(all.data(), dn, all.size(), cudaMemcpyDeviceToHost, st));
         XB_CUDA(cudaStreamSynchronize(st));

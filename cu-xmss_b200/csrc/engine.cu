@@ -284,9 +284,19 @@ static void run_ltree(const FamilyOps* ops, const LeafRef* refs, uint32_t nslots
 }
 
 void Engine::build_trees(const FamilyOps* ops, const TreeJob* d_jobs, uint32_t njobs, int h, uint8_t* d_nodes,
-                         const void* d_ctx, cudaStream_t st, Workspace& w)
+                         const void* d_ctx, cudaStream_t st, Workspace& w, int subtree_k)
 {
     const bool on = &w == &ws_;  // server workspaces record no marks
+    if (subtree_k >= 5 && subtree_k <= 7 && subtree_k <= h) {
+        // levels 0..k in one launch of in-CTA subtrees, the rest across CTAs
+        mark(kChains, true, st, on);
+        ops->keygen_subtree(d_jobs, njobs, h, subtree_k, d_ctx, d_nodes, st);
+        mark(kChains, false, st, on);
+        mark(kTree, true, st, on);
+        for (int level = subtree_k; level < h; level++) ops->tree_level(d_jobs, njobs, h, level, d_nodes, d_ctx, st);
+        mark(kTree, false, st, on);
+        return;
+    }
     const uint64_t total = (uint64_t)njobs << h;
     const uint64_t per_slot = (uint64_t)ops->len * ops->n;
     const uint64_t cap = std::max<uint64_t>(1, std::min<uint64_t>(total, kChainScratchBytes / per_slot));
@@ -320,7 +330,7 @@ void Engine::keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count,
     TreeJob* dj = w.jobs.as<TreeJob>(count);
     XB_CUDA(cudaMemcpyAsync(dj, hj, count * sizeof(TreeJob), cudaMemcpyHostToDevice, st));
     uint8_t* nodes = w.nodes.as<uint8_t>(count * tree_bytes);
-    build_trees(ops, dj, count, (int)th, nodes, ctx, st, w);
+    build_trees(ops, dj, count, (int)th, nodes, ctx, st, w, subtree_k(p, count));
     k_keypair_finish<<<count, 64, 0, st>>>(d_seeds, nodes, tree_bytes, level_offset((int)th, (int)th) * n, n,
                                           p.index_bytes, (uint32_t)p.sk_bytes, count, d_pk, d_sk);
     // the host job list is reused by the next call only after this one's
@@ -489,24 +499,28 @@ void Engine::verify_persistent(const FamilyOps* ops, const xmss_params& p, uint3
     v.tree_height = p.tree_height;
     v.d = d;
     // state: ticket (8 B), header, then per (group, layer) ready / ntot /
-    // chains_done / 8 L-tree level counters, then per group h_pre counters
+    // chains_done / 8 L-tree level counters, per group h_pre counters, and
+    // the H_msg length histogram and bucket cursors
     const size_t gl = (size_t)groups * d;
-    const size_t words = 4 + gl * 11 + groups;
+    const size_t words = kPersistHdrWords + gl * 11 + groups + 2 * kSortBuckets;
     uint8_t* st8 = w.pstate.as<uint8_t>(8 + words * 4);
     uint32_t* u = (uint32_t*)(st8 + 8);
     PersistArgs q{};
     q.ticket = (unsigned long long*)st8;
     q.hdr = u;
-    q.ready = u + 4;
+    q.ready = u + kPersistHdrWords;
     q.ntot = q.ready + gl;
     q.chains_done = q.ntot + gl;
     q.lt_done = q.chains_done + gl;
     q.hpre_done = q.lt_done + 8 * gl;
+    q.sort = q.hpre_done + groups;
+    q.perm = w.aux.as<uint32_t>(count);
     q.list = w.list.as<uint32_t>((size_t)groups * 32 * len);
     q.ctx = w.ctx.get((size_t)npk * ops->ctx_bytes);
     q.npk = npk;
     q.groups = groups;
     q.wait_ns = persist_wait_ns;
+    q.short_blocks = tuning_for(ops->func, ops->n).short_hmsg_blocks;
     XB_CUDA(cudaMemsetAsync(st8, 0, 8 + words * 4, st));
     ops->verify_persist(v, q, st);
     XB_CUDA(cudaGetLastError());
@@ -579,7 +593,7 @@ void Engine::sign(const FamilyOps* ops, const xmss_params& p, uint32_t count, co
     // key material rows: SK_SEED | SK_PRF | root | PUB_SEED
     ops->make_ctx(dkeys + 3 * n, 4 * n, dkeys, 4 * n, dkeys + n, 4 * n, nkeys, ctx, st);
     uint8_t* nodes = w.nodes.as<uint8_t>(njobs * tree_bytes);
-    build_trees(ops, (const TreeJob*)(ds + o_jobs), njobs, (int)th, nodes, ctx, st, w);
+    build_trees(ops, (const TreeJob*)(ds + o_jobs), njobs, (int)th, nodes, ctx, st, w, subtree_k(p, njobs));
     SignArgs g;
     g.sm = d_sm;
     g.sm_off = d_sm_off;

@@ -138,12 +138,16 @@ class Engine {
     // -- pipelines (device pointers, asynchronous on st) ---------------------
     // Builds every subtree of `jobs` (all of height h): node arrays at
     // d_nodes + job.node_off, levels 0..h.  d_jobs is the device copy of jobs.
+    // subtree_k 0: one thread per chain and a launch per level; 5..7: levels
+    // 0..k as in-CTA subtrees (subtree_height_for gives it per parameter set).
     void build_trees(const FamilyOps* ops, const TreeJob* d_jobs, uint32_t njobs, int h, uint8_t* d_nodes,
-                     const void* d_ctx, cudaStream_t st, Workspace& w);
-    void build_trees(const FamilyOps* ops, const TreeJob* d_jobs, uint32_t njobs, int h, uint8_t* d_nodes,
-                     const void* d_ctx, cudaStream_t st)
+                     const void* d_ctx, cudaStream_t st, Workspace& w, int subtree_k = 0);
+
+    // The in-CTA subtree height for a build of njobs subtrees of parameter set p.
+    static int subtree_k(const xmss_params& p, uint32_t njobs)
     {
-        build_trees(ops, d_jobs, njobs, h, d_nodes, d_ctx, st, ws_);
+        const TreeShape& s = tree_shape_for(p.func, p.n, p.full_height, p.d);
+        return subtree_height_for(s, (int)p.tree_height, (uint64_t)njobs << p.tree_height);
     }
 
     // Verify of `count` signed messages against npk public keys (root||seed).

@@ -2,6 +2,8 @@
 // table.  Included by exactly one fam_*.cu per family.
 #pragma once
 
+#include <algorithm>
+
 #include "family_ops.h"
 #include "verify_persist.cuh"
 #include "xmss_kernels.cuh"
@@ -80,6 +82,23 @@ struct Launch {
         if (!items) return;
         const unsigned b = tune().level_block;
         k_tree_level<F><<<grid_for(items, b), b, 0, st>>>(jobs, njobs, h, level, nodes, (const Ctx*)ctx);
+    }
+    static void keygen_subtree(const TreeJob* jobs, uint32_t njobs, int h, int k, const void* ctx, uint8_t* nodes,
+                               cudaStream_t st)
+    {
+        if (!njobs || k < 1 || k > 7 || k > h) return;
+        const unsigned b = 1u << k;
+        // opt in to more than 48 KB of dynamic shared memory where the
+        // widest family needs it (n = 64: 80 KB at 128 threads)
+        static const bool attr = [] {
+            return cudaFuncSetAttribute(k_keygen_subtree<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)subtree_smem<FT>(128)) == cudaSuccess;
+        }();
+        (void)attr;
+        const uint64_t ctas = (uint64_t)njobs << (h - k);
+        for (uint64_t c0 = 0; c0 < ctas; c0 += 1u << 30)
+            k_keygen_subtree<FT><<<(unsigned)std::min<uint64_t>(ctas - c0, 1u << 30), b, subtree_smem<FT>(b), st>>>(
+                jobs, h, k, c0, (const typename FT::Ctx*)ctx, nodes);
     }
     static void verify_partition(const VerifyArgs& v, uint32_t blocks_max, uint32_t* sel_short, uint32_t* sel_long,
                                  uint32_t* n2, cudaStream_t st)
@@ -192,6 +211,7 @@ struct Launch {
         o.keygen_chains = keygen_chains;
         o.ltree_level = ltree_level;
         o.tree_level = tree_level;
+        o.keygen_subtree = keygen_subtree;
         o.hpre_bytes = sizeof(typename F::HPre);
         o.verify_partition = verify_partition;
         o.verify_prep = verify_prep;

@@ -28,6 +28,9 @@ struct FamilyOps {
                         const int* status, cudaStream_t st);
     void (*tree_level)(const TreeJob* jobs, uint32_t njobs, int h, int level, uint8_t* nodes, const void* ctx,
                        cudaStream_t st);
+    // levels 0..k of every job's tree as in-CTA subtrees of 2^k leaves, one thread per leaf (k = 5, 6, 7; k <= h)
+    void (*keygen_subtree)(const TreeJob* jobs, uint32_t njobs, int h, int k, const void* ctx, uint8_t* nodes,
+                           cudaStream_t st);
     size_t hpre_bytes;  // sizeof(F::HPre)
     void (*verify_partition)(const VerifyArgs& v, uint32_t blocks_max, uint32_t* sel_short, uint32_t* sel_long,
                              uint32_t* n2, cudaStream_t st);
@@ -62,6 +65,19 @@ struct Tuning {
     uint32_t prep_split = 1;            // split batches: h_pre in its own launch (1) or in each group's prep (0)
 };
 Tuning& tuning_for(unsigned func, unsigned n);
+
+// How subtrees of one parameter set are built (set by the autotuner, tune.cu;
+// keyed by the parameter set, i.e. its OID).
+struct TreeShape {
+    uint32_t subtree_height = 0;  // 0: one thread per WOTS chain, a launch per L-tree / Merkle level;
+                                  // 5, 6, 7: in-CTA subtrees of 2^k leaves, one thread per leaf
+    uint64_t min_leaves = 0;      // builds of fewer leaves use the one-thread-per-chain form
+};
+TreeShape& tree_shape_for(unsigned func, unsigned n, unsigned full_height, unsigned d);
+
+// The in-CTA subtree height to build `leaves` leaves of subtrees of height
+// h with (0: the one-thread-per-chain form).
+int subtree_height_for(const TreeShape& s, int h, uint64_t leaves);
 
 extern const FamilyOps kOpsSha256N32;
 extern const FamilyOps kOpsSha256N24;

@@ -124,6 +124,111 @@ __device__ __forceinline__ void sha256_compress_t(uint32_t (&st)[8], uint32_t (&
     st[4] += e; st[5] += f; st[6] += g; st[7] += h;
 }
 
+// Rotations on the FMA pipe.  x * 2^(32-k) is a 64-bit product whose high
+// word is x >> k and whose low word is x << (32-k); the two have no bit in
+// common, so their sum is rotr(x, k).  The power of two comes from constant
+// memory, so the multiplies stay multiplies (IMAD) instead of becoming
+// shifts (ALU pipe).
+template <int K>
+__device__ __forceinline__ uint32_t fma_ror(uint32_t x)
+{
+    uint32_t lo, r;
+    asm("mul.lo.u32 %0, %1, %2;" : "=r"(lo) : "r"(x), "r"(xb_pipe_pow2[32 - K]));
+    asm("mad.hi.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(xb_pipe_pow2[32 - K]), "r"(lo));
+    return r;
+}
+
+template <int K>
+__device__ __forceinline__ uint32_t fma_ror_wide(uint32_t x)
+{
+    uint32_t lo, hi;
+    asm("{\n\t.reg .u64 t;\n\tmul.wide.u32 t, %2, %3;\n\tmov.b64 {%0, %1}, t;\n\t}"
+        : "=r"(lo), "=r"(hi)
+        : "r"(x), "r"(xb_pipe_pow2[32 - K]));
+    return fma_add(lo, hi);
+}
+
+// SHA-256 compression with more of the ALU work moved to the FMA pipe than
+// sha256_compress_t<1> (compare with the rate probe; results identical):
+//   4  the schedule's w[t-16] + w[t-7] and the final state additions too
+//   5  4, and one rotation of each of S0 and S1 as fma_ror
+//   6  4, and the same rotations as fma_ror_wide
+//   7  5, and h + K[t] + W[t] as two multiply-adds
+//   8  5, and the schedule's shifts (fma_shr) and one rotation of each of
+//      s0 and s1 as fma_ror
+//   9  4, and every rotation of S0 and S1 as fma_ror
+template <int MIX>
+__device__ __forceinline__ void sha256_compress_x(uint32_t (&st)[8], uint32_t (&w)[16])
+{
+    const uint32_t K[64] = {
+        0x428a2f98u, 0x71374491u, 0xb5c0fbcfu, 0xe9b5dba5u, 0x3956c25bu, 0x59f111f1u,
+        0x923f82a4u, 0xab1c5ed5u, 0xd807aa98u, 0x12835b01u, 0x243185beu, 0x550c7dc3u,
+        0x72be5d74u, 0x80deb1feu, 0x9bdc06a7u, 0xc19bf174u, 0xe49b69c1u, 0xefbe4786u,
+        0x0fc19dc6u, 0x240ca1ccu, 0x2de92c6fu, 0x4a7484aau, 0x5cb0a9dcu, 0x76f988dau,
+        0x983e5152u, 0xa831c66du, 0xb00327c8u, 0xbf597fc7u, 0xc6e00bf3u, 0xd5a79147u,
+        0x06ca6351u, 0x14292967u, 0x27b70a85u, 0x2e1b2138u, 0x4d2c6dfcu, 0x53380d13u,
+        0x650a7354u, 0x766a0abbu, 0x81c2c92eu, 0x92722c85u, 0xa2bfe8a1u, 0xa81a664bu,
+        0xc24b8b70u, 0xc76c51a3u, 0xd192e819u, 0xd6990624u, 0xf40e3585u, 0x106aa070u,
+        0x19a4c116u, 0x1e376c08u, 0x2748774cu, 0x34b0bcb5u, 0x391c0cb3u, 0x4ed8aa4au,
+        0x5b9cca4fu, 0x682e6ff3u, 0x748f82eeu, 0x78a5636fu, 0x84c87814u, 0x8cc70208u,
+        0x90befffau, 0xa4506cebu, 0xbef9a3f7u, 0xc67178f2u};
+    static_assert(MIX >= 4 && MIX <= 9, "pipe mix");
+    uint32_t a = st[0], b = st[1], c = st[2], d = st[3];
+    uint32_t e = st[4], f = st[5], g = st[6], h = st[7];
+#pragma unroll
+    for (int t = 0; t < 64; t++) {
+        if (t >= 16) {
+            const uint32_t x15 = w[(t - 15) & 15], x2 = w[(t - 2) & 15];
+            uint32_t s0, s1;
+            if constexpr (MIX == 8) {
+                s0 = fma_ror<7>(x15) ^ ror32(x15, 18) ^ fma_shr<3>(x15);
+                s1 = fma_ror<17>(x2) ^ ror32(x2, 19) ^ fma_shr<10>(x2);
+            } else {
+                s0 = ror32(x15, 7) ^ ror32(x15, 18) ^ (x15 >> 3);
+                s1 = ror32(x2, 17) ^ ror32(x2, 19) ^ (x2 >> 10);
+            }
+            w[t & 15] = fma_add(s1, fma_add(s0, fma_add(w[t & 15], w[(t - 7) & 15])));
+        }
+        uint32_t S1, S0;
+        if constexpr (MIX == 5 || MIX == 7 || MIX == 8) {
+            S1 = fma_ror<6>(e) ^ ror32(e, 11) ^ ror32(e, 25);
+            S0 = fma_ror<2>(a) ^ ror32(a, 13) ^ ror32(a, 22);
+        } else if constexpr (MIX == 6) {
+            S1 = fma_ror_wide<6>(e) ^ ror32(e, 11) ^ ror32(e, 25);
+            S0 = fma_ror_wide<2>(a) ^ ror32(a, 13) ^ ror32(a, 22);
+        } else if constexpr (MIX == 9) {
+            S1 = fma_ror<6>(e) ^ fma_ror<11>(e) ^ fma_ror<25>(e);
+            S0 = fma_ror<2>(a) ^ fma_ror<13>(a) ^ fma_ror<22>(a);
+        } else {
+            S1 = ror32(e, 6) ^ ror32(e, 11) ^ ror32(e, 25);
+            S0 = ror32(a, 2) ^ ror32(a, 13) ^ ror32(a, 22);
+        }
+        const uint32_t ch = g ^ (e & (f ^ g));
+        const uint32_t mj = (a & b) | (c & (a | b));
+        uint32_t hkw;
+        if constexpr (MIX == 7) {
+            hkw = fma_add(h, fma_add(w[t & 15], K[t]));
+        } else {
+            hkw = h + K[t] + w[t & 15];
+        }
+        const uint32_t t1 = fma_add(ch, fma_add(S1, hkw));
+        h = g; g = f; f = e; e = fma_add(d, t1);
+        d = c; c = b; b = a; a = fma_add(S0, fma_add(mj, t1));
+    }
+    st[0] = fma_add(st[0], a); st[1] = fma_add(st[1], b); st[2] = fma_add(st[2], c); st[3] = fma_add(st[3], d);
+    st[4] = fma_add(st[4], e); st[5] = fma_add(st[5], f); st[6] = fma_add(st[6], g); st[7] = fma_add(st[7], h);
+}
+
+template <int MIX>
+__device__ __forceinline__ void sha256_compress_any(uint32_t (&st)[8], uint32_t (&w)[16])
+{
+    if constexpr (MIX >= 4) {
+        sha256_compress_x<MIX>(st, w);
+    } else {
+        sha256_compress_t<MIX>(st, w);
+    }
+}
+
 __device__ __forceinline__ void sha256_compress(uint32_t (&st)[8], uint32_t (&w)[16])
 {
     sha256_compress_t<XB_SHA256_MIX>(st, w);

@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(128) k_sha256_rate(uint32_t iters, uint32_t se
             w[j] = st[j];
             w[8 + j] = st[j] ^ i;
         }
-        sha256_compress_t<MIX>(st, w);
+        sha256_compress_any<MIX>(st, w);
     }
     uint32_t x = 0;
 #pragma unroll
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(128) k_sha512_rate(uint32_t iters, uint32_t se
 
 // kind 0: SHA-256 as the XMSS kernels compile it; 1: Keccak-f[1600];
 // 2: SHA-512 compressions;
-// 10 + m: SHA-256 with pipe mix m (for comparing the variants);
+// 10 + m: SHA-256 with pipe mix m, 0..9 (for comparing the variants);
 // 20 + m: the same with one warp per block (latency of a lone thread).
 void launch_rate(int kind, uint32_t blocks, uint32_t iters, uint32_t* sink, cudaStream_t st)
 {
@@ -90,6 +90,12 @@ void launch_rate(int kind, uint32_t blocks, uint32_t iters, uint32_t* sink, cuda
         case 10: k_sha256_rate<0><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
         case 11: k_sha256_rate<1><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
         case 12: k_sha256_rate<2><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 14: k_sha256_rate<4><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 15: k_sha256_rate<5><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 16: k_sha256_rate<6><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 17: k_sha256_rate<7><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 18: k_sha256_rate<8><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
+        case 19: k_sha256_rate<9><<<blocks, 128, 0, st>>>(iters, 0x1234567u, sink); break;
         default: break;
     }
 }

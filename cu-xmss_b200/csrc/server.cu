@@ -740,7 +740,8 @@ Launch xmss_b200_server::launch(Slot& s, std::vector<std::unique_ptr<Request>>& 
             } else {
                 if (!pl.jobs.empty()) {
                     engine->build_trees(pl.ops, (const TreeJob*)(d + pl.o_jobs), (uint32_t)pl.jobs.size(),
-                                        (int)p.tree_height, pool.as<uint8_t>(0), pl.table->ctx.as<uint8_t>(0), L.st, L.w);
+                                        (int)p.tree_height, pool.as<uint8_t>(0), pl.table->ctx.as<uint8_t>(0), L.st, L.w,
+                                        xb::Engine::subtree_k(p, (uint32_t)pl.jobs.size()));
                     for (const TreeId& id : pl.job_ids) XB_CUDA(cudaEventRecord(trees[id].ready, L.st));
                 }
                 for (const TreeId& id : pl.used) {  // subtrees other slots are still building

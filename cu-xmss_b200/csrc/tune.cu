@@ -18,7 +18,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <random>
+#include <tuple>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -37,6 +40,22 @@ Tuning& tuning_for(unsigned func, unsigned n)
     const unsigned f = func < 3 ? func : 0;
     const unsigned i = n == 24 ? 0 : (n == 64 ? 2 : 1);
     return table[f][i];
+}
+
+TreeShape& tree_shape_for(unsigned func, unsigned n, unsigned full_height, unsigned d)
+{
+    // (func, n, full height, layers) names one parameter set of params.c
+    static std::mutex mu;
+    static std::map<std::tuple<unsigned, unsigned, unsigned, unsigned>, TreeShape> table;
+    std::lock_guard<std::mutex> g(mu);
+    return table[std::make_tuple(func, n, full_height, d)];
+}
+
+int subtree_height_for(const TreeShape& s, int h, uint64_t leaves)
+{
+    const int k = (int)s.subtree_height;
+    if (k < 5 || k > 7 || leaves < s.min_leaves) return 0;
+    return h >= k ? k : (h >= 5 ? h : 0);
 }
 }  // namespace xb
 
@@ -80,6 +99,40 @@ extern "C" int xmss_b200_tuning_set(unsigned func, unsigned n, const xmss_b200_t
     d.split_min = t->split_min;
     d.short_hmsg_blocks = t->short_hmsg_blocks;
     d.prep_split = t->prep_split;
+    return 0;
+}
+
+namespace {
+
+xb::TreeShape* shape_of(uint32_t oid, int mt, xmss_params* p)
+{
+    if ((mt ? xmssmt_parse_oid(p, oid) : xmss_parse_oid(p, oid)) != 0 || !xb::family_ops(p->func, p->n)) return nullptr;
+    return &xb::tree_shape_for(p->func, p->n, p->full_height, p->d);
+}
+
+}  // namespace
+
+extern "C" int xmss_b200_tree_tuning_get(uint32_t oid, int mt, xmss_b200_tree_tuning* out)
+{
+    xmss_params p;
+    const xb::TreeShape* s = shape_of(oid, mt, &p);
+    if (!s || !out) return -1;
+    out->subtree_height = s->subtree_height;
+    out->chains_per_warp = s->subtree_height ? 32 * p.wots_len : 32;
+    out->min_leaves = s->min_leaves;
+    return 0;
+}
+
+extern "C" int xmss_b200_tree_tuning_set(uint32_t oid, int mt, const xmss_b200_tree_tuning* t)
+{
+    xmss_params p;
+    xb::TreeShape* s = shape_of(oid, mt, &p);
+    if (!s || !t || (t->subtree_height != 0 && (t->subtree_height < 5 || t->subtree_height > 7))) {
+        xb::set_last_error("xmss_b200_tree_tuning_set: unknown OID or subtree height other than 0, 5, 6, 7");
+        return -1;
+    }
+    s->subtree_height = t->subtree_height;
+    s->min_leaves = t->min_leaves;
     return 0;
 }
 
@@ -312,6 +365,131 @@ extern "C" int xmss_b200_autotune(uint32_t oid, int mt, uint32_t count, xmss_b20
         rep += line;
     } catch (const std::exception& ex) {
         xb::set_last_error(std::string("xmss_b200_autotune: ") + ex.what());
+        return -3;
+    }
+    if (report && report_cap) {
+        const size_t k = std::min(report_cap - 1, rep.size());
+        memcpy(report, rep.data(), k);
+        report[k] = 0;
+    }
+    return 0;
+}
+
+// Tree-building shape of one parameter set: keygen of slices of 2^12, 2^15
+// and 2^18 leaves (subtrees of the set's height, seeded keys, L2 flushed
+// before each timed run, median of five), one thread per chain against
+// in-CTA subtrees of height 5, 6 and 7; every candidate's node arrays must
+// equal those of the one-thread-per-chain form.  The best in-CTA height at
+// the largest slice is kept if it is at least 2 % faster there, with
+// min_leaves = the smallest slice at which it still is.
+extern "C" int xmss_b200_autotune_tree(uint32_t oid, int mt, xmss_b200_tree_tuning* best, char* report,
+                                       size_t report_cap)
+{
+    xmss_params p;
+    xb::TreeShape* shape = shape_of(oid, mt, &p);
+    if (!shape) {
+        xb::set_last_error("xmss_b200_autotune_tree: unknown OID");
+        return -1;
+    }
+    std::string rep;
+    try {
+        xb::Engine& e = xb::Engine::get();
+        std::lock_guard<std::mutex> lk(e.mu);
+        XB_CUDA(cudaSetDevice(e.device()));
+        const xb::FamilyOps* ops = xb::ops_for(p);
+        cudaStream_t st = e.stream();
+        xb::Workspace w;
+        const size_t n = p.n;
+        const int h = (int)p.tree_height;
+        constexpr uint32_t nk = 4;
+        std::mt19937_64 rng(0x7EE5ull ^ oid ^ ((uint64_t)mt << 32));
+        std::vector<uint8_t> mat((size_t)nk * 4 * n);
+        for (auto& b : mat) b = (uint8_t)rng();
+        xb::DevBuf d_mat, d_ctx, d_jobs, d_nodes, d_ref, flush;
+        XB_CUDA(cudaMemcpy(d_mat.get(mat.size()), mat.data(), mat.size(), cudaMemcpyHostToDevice));
+        uint8_t* dm = d_mat.as<uint8_t>(0);
+        void* ctx = d_ctx.get((size_t)nk * ops->ctx_bytes);
+        ops->make_ctx(dm + 3 * n, 4 * n, dm, 4 * n, dm + n, 4 * n, nk, ctx, st);
+        void* fl = flush.get(256ull << 20);
+        cudaEvent_t a, b;
+        XB_CUDA(cudaEventCreate(&a));
+        XB_CUDA(cudaEventCreate(&b));
+        char line[256];
+        rep = "{\"oid\": " + std::to_string(oid) + ", \"mt\": " + std::to_string(mt) + ", \"trials\": [";
+        bool first = true;
+        const int sizes[3] = {12, 15, 18};
+        double t_at[3][8] = {};
+        for (int si = 0; si < 3; si++) {
+            const int lg = std::max(sizes[si], h);  // at least one subtree
+            const uint32_t njobs = 1u << (lg - h);
+            const uint64_t tree_bytes = ((2ull << h) - 1) * n;
+            std::vector<xb::TreeJob> jobs(njobs);
+            for (uint32_t j = 0; j < njobs; j++) jobs[j] = xb::TreeJob{j % nk, 0, j / nk, j * tree_bytes};
+            XB_CUDA(cudaMemcpy(d_jobs.get(njobs * sizeof(xb::TreeJob)), jobs.data(), njobs * sizeof(xb::TreeJob),
+                               cudaMemcpyHostToDevice));
+            const size_t bytes = (size_t)njobs * tree_bytes;
+            uint8_t* nodes = d_nodes.as<uint8_t>(bytes);
+            uint8_t* ref = d_ref.as<uint8_t>(bytes);
+            std::vector<uint8_t> h_ref(bytes), h_got(bytes);
+            for (int k : {0, 5, 6, 7}) {
+                if (k > h) continue;
+                auto run = [&] {
+                    e.build_trees(ops, d_jobs.as<xb::TreeJob>(0), njobs, h, nodes, ctx, st, w, k);
+                };
+                run();
+                std::vector<float> t;
+                for (int i = 0; i < 5; i++) {
+                    XB_CUDA(cudaMemsetAsync(fl, i, 256ull << 20, st));
+                    XB_CUDA(cudaEventRecord(a, st));
+                    run();
+                    XB_CUDA(cudaEventRecord(b, st));
+                    XB_CUDA(cudaEventSynchronize(b));
+                    float ms = 0;
+                    XB_CUDA(cudaEventElapsedTime(&ms, a, b));
+                    t.push_back(ms);
+                }
+                std::sort(t.begin(), t.end());
+                t_at[si][k] = t[2];
+                if (k == 0) {
+                    XB_CUDA(cudaMemcpy(h_ref.data(), nodes, bytes, cudaMemcpyDeviceToHost));
+                } else {
+                    XB_CUDA(cudaMemcpy(h_got.data(), nodes, bytes, cudaMemcpyDeviceToHost));
+                    if (h_got != h_ref) throw std::runtime_error("in-CTA subtrees differ from the per-chain form");
+                }
+                snprintf(line, sizeof line, "%s{\"leaves_log2\": %d, \"subtree_height\": %d, \"ms\": %.4f}",
+                         first ? "" : ", ", lg, k, (double)t[2]);
+                rep += line;
+                first = false;
+            }
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        constexpr double kGain = 0.98;
+        int kb = 0;
+        for (int k : {5, 6, 7})
+            if (k <= h && t_at[2][k] > 0 && t_at[2][k] < kGain * t_at[2][0] &&
+                (kb == 0 || t_at[2][k] < t_at[2][kb]))
+                kb = k;
+        uint64_t min_leaves = 0;
+        if (kb) {
+            min_leaves = 1ull << std::max(sizes[2], h);
+            for (int si = 1; si >= 0; si--) {
+                if (t_at[si][kb] > 0 && t_at[si][kb] < kGain * t_at[si][0])
+                    min_leaves = 1ull << std::max(sizes[si], h);
+                else
+                    break;
+            }
+        }
+        shape->subtree_height = (uint32_t)kb;
+        shape->min_leaves = min_leaves;
+        xmss_b200_tree_tuning out;
+        xmss_b200_tree_tuning_get(oid, mt, &out);
+        if (best) *best = out;
+        snprintf(line, sizeof line, "], \"best\": {\"subtree_height\": %u, \"chains_per_warp\": %u, \"min_leaves\": %llu}}",
+                 out.subtree_height, out.chains_per_warp, (unsigned long long)out.min_leaves);
+        rep += line;
+    } catch (const std::exception& ex) {
+        xb::set_last_error(std::string("xmss_b200_autotune_tree: ") + ex.what());
         return -3;
     }
     if (report && report_cap) {

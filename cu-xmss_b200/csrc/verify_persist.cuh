@@ -7,17 +7,29 @@
 // tickets.  Signatures are taken in groups of 32 (one per lane), and each
 // warp pops one ticket at a time:
 //
-//   ctx      32 keys: the PUB_SEED midstates                       (no deps)
+//   count    1,024 signatures: histogram of their H_msg block counts  (no deps)
+//   ctx      32 keys: the PUB_SEED midstates                         (no deps)
+//   prefix   bucket offsets of the histogram, longest H_msg first      (count)
+//   scatter  1,024 signatures: their places in that order (perm)       (prefix)
 //   hmsg     one group: H_msg + base_w (lane = signature), then the
-//            group's chains bucketed longest first into its list   (no deps)
+//            group's chains bucketed longest first into its list   (scatter)
 //   hpre     one group, one H node of one layer: h_pre             (ctx)
 //   per layer l:
-//     chain  32 list entries of one group (entry c*32 .. c*32+31),
-//            tickets ordered by c so the longest chains go first  (list of g, l)
+//     chain  32 list entries of one group (entry c*32 .. c*32+31)  (list of g, l)
 //     ltree  one L-tree pair index of one level for the group      (chains, h_pre /
 //                                                                   level before)
 //     root   compute_root of the group; then the next layer's
 //            chain list, or the comparison with the public root    (last level)
+//
+// Group g holds the signatures perm[32g .. 32g + 31]: the batch sorted by
+// H_msg length, longest first, so a group's chains wait only for messages of
+// about the same length.  The hmsg tickets run in that order (the long,
+// serial H_msg start first); the tasks after them run in the reverse order,
+// shortest H_msg first, so that the first chain tickets find their lists
+// ready.  Chain tickets are taken in two bands, like the two-stream split of
+// the multi-launch pipeline: the groups whose H_msg is at most short_blocks
+// hash blocks, then the longer ones; inside a band they go by list position
+// c, so the longest chains of every group go first.
 //
 // A warp waits for a task's inputs by polling a per-group counter that the
 // producing tasks increment.  Since every producer holds a smaller ticket,
@@ -37,26 +49,39 @@
 
 namespace xb {
 
+// Buckets of the H_msg length sort (block counts at or above the last one
+// share it) and signatures per count / scatter task.
+constexpr uint32_t kSortBuckets = 1024;
+constexpr uint32_t kSortChunk = 1024;
+
 // State of one persistent launch.  Zeroed before the launch.
 struct PersistArgs {
     unsigned long long* ticket;  // next ticket
-    uint32_t* hdr;               // [0] error flag, [1] CTAs exited, [2] ctx tasks done
+    uint32_t* hdr;               // [0] error flag, [1] CTAs exited, [2] ctx tasks done, [3] count tasks
+                                 // done, [4] prefix done, [5] scatter tasks done, [6] long signatures
     uint32_t* ready;             // [G*d] chain list of (group, layer) written
     uint32_t* ntot;              // [G*d] chains in that list
     uint32_t* chains_done;       // [G*d] chain tasks finished
     uint32_t* lt_done;           // [G*d*8] L-tree level tasks finished
     uint32_t* hpre_done;         // [G] h_pre tasks finished
     uint32_t* list;              // [G][32*LEN] chain items (s*LEN + chain) of the group's current layer
+    uint32_t* perm;              // [count] signatures in group order
+    uint32_t* sort;              // [2 * kSortBuckets] histogram, then bucket cursors
     void* ctx;                   // [npk] F::Ctx, written by the ctx tasks
     unsigned long long wait_ns;  // bound of one dependency wait (%globaltimer ns)
     uint32_t npk;
     uint32_t groups;
+    uint32_t short_blocks;       // chain band boundary: H_msg hash blocks of a short group
 };
+
+// Header words of a PersistArgs state block.
+constexpr uint32_t kPersistHdrWords = 8;
 
 // Default bound of a single dependency wait (ns of %globaltimer).  Inputs of
 // a task are produced by tasks already running, so a legitimate wait lasts at
 // most about one H_msg: 8 s is a message of several hundred MB.
 constexpr unsigned long long kPersistWaitNs = 8000000000ull;
+
 
 // L-tree shape (xmss_commons.c:16-49): level l reduces cnt(l) nodes into
 // items(l) = ceil(cnt/2) (the odd node is carried up); its hashed pairs are
@@ -220,6 +245,27 @@ constexpr int persist_min_ctas()
     return HMsgKind<F>::v == 0 ? 5 : 2;
 }
 
+
+// Sort bucket of a signature: longer H_msg first; signatures that are
+// rejected before H_msg (too short) last.
+template <class F>
+__device__ __forceinline__ uint32_t persist_sort_bucket(const VerifyArgs& v, uint32_t s)
+{
+    const uint64_t smlen = v.smlen[s];
+    if (smlen < v.sig_bytes) return kSortBuckets - 1;
+    const unsigned long long b = hmsg_blocks<F>(smlen - v.sig_bytes);
+    return kSortBuckets - 1 - (uint32_t)(b < kSortBuckets - 1 ? b : kSortBuckets - 1);
+}
+
+// Tasks of one persistent verify (the ticket count of its launch).
+__host__ __device__ inline unsigned long long persist_verify_tasks(uint32_t count, uint32_t npk, uint32_t d,
+                                                                   uint32_t th, int len)
+{
+    const unsigned long long G = (count + 31) / 32, K = (npk + 31) / 32, S = (count + kSortChunk - 1) / kSortChunk;
+    const unsigned long long nh = (unsigned long long)len - 1 + th;
+    return 2 * S + 1 + K + G + G * d * nh + (unsigned long long)d * G * (len + lt_items_total(len) + 1);
+}
+
 // F runs every task except the chains, which run FT (same family, another
 // pipe mix; the key context is shared).
 template <class F, class FT>
@@ -234,12 +280,22 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
     uint32_t* cnt = sh_cnt[(threadIdx.x >> 5) & 3];
     uint32_t* err = q.hdr;
     Ctx* ctx = (Ctx*)q.ctx;
-    const uint32_t G = q.groups, d = v.d, th = v.tree_height;
+    const uint32_t G = q.groups, d = v.d, th = v.tree_height, count = v.count;
     const uint32_t nh = LEN - 1 + th;
     const unsigned long long K = (q.npk + 31) / 32;
+    const unsigned long long S = (count + kSortChunk - 1) / kSortChunk;
     const unsigned long long n_hpre = (unsigned long long)G * d * nh;
     const unsigned long long per_layer = (unsigned long long)G * (LEN + LT + 1);
-    const unsigned long long total = K + G + n_hpre + per_layer * d;
+    const unsigned long long total = persist_verify_tasks(count, q.npk, d, th, LEN);
+    uint32_t* hist = q.sort;
+    uint32_t* cursor = q.sort + kSortBuckets;
+    // signature of lane `lane` in group g (count: none)
+    auto sig_of = [&](uint32_t g) -> uint32_t {
+        const uint32_t i = g * 32 + lane;
+        return i < count ? q.perm[i] : count;
+    };
+    // the group at position `pos` of the readiness order (shortest H_msg first)
+    auto group_at = [&](uint32_t pos) -> uint32_t { return G - 1 - pos; };
 
     for (;;) {
         unsigned long long t = 0;
@@ -247,6 +303,15 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= total || *(volatile uint32_t*)err) break;
 
+        if (t < S) {  // -------- count: H_msg length histogram of 1,024 signatures
+            for (uint32_t i = lane; i < kSortChunk; i += 32) {
+                const uint32_t s = (uint32_t)t * kSortChunk + i;
+                if (s < count) atomicAdd(&hist[persist_sort_bucket<F>(v, s)], 1u);
+            }
+            persist_signal(&q.hdr[3]);
+            continue;
+        }
+        t -= S;
         if (t < K) {  // -------- ctx: 32 keys
             const uint32_t k = (uint32_t)t * 32 + lane;
             if (k < q.npk) {
@@ -258,10 +323,52 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
             continue;
         }
         t -= K;
-        if (t < G) {  // -------- H_msg + base_w of one group, then its layer-0 list
-            const uint32_t g = (uint32_t)t, s = g * 32 + lane;
+        if (t == 0) {  // -------- prefix: bucket cursors (exclusive prefix sums), long signatures
+            if (!persist_wait(&q.hdr[3], (uint32_t)S, err, q.wait_ns)) break;
+            constexpr uint32_t per = kSortBuckets / 32;
+            uint32_t sum = 0;
+            for (uint32_t j = 0; j < per; j++) sum += ld_relaxed(&hist[lane * per + j]);
+            uint32_t incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if ((int)lane >= o) incl += y;
+            }
+            uint32_t run = incl - sum;
+            for (uint32_t j = 0; j < per; j++) {
+                const uint32_t b = lane * per + j;
+                cursor[b] = run;
+                run += ld_relaxed(&hist[b]);
+            }
+            __syncwarp();
+            // signatures with more than short_blocks H_msg blocks come before
+            // bucket kSortBuckets - 1 - short_blocks
+            const uint32_t cut = kSortBuckets - 1 - (q.short_blocks < kSortBuckets - 1 ? q.short_blocks : kSortBuckets - 1);
+            if (lane == cut / per) {
+                uint32_t c = incl - sum;
+                for (uint32_t b = lane * per; b < cut; b++) c += ld_relaxed(&hist[b]);
+                q.hdr[6] = c;
+            }
+            persist_signal(&q.hdr[4]);
+            continue;
+        }
+        t -= 1;
+        if (t < S) {  // -------- scatter: places of 1,024 signatures in group order
+            if (!persist_wait(&q.hdr[4], 1u, err, q.wait_ns)) break;
+            for (uint32_t i = lane; i < kSortChunk; i += 32) {
+                const uint32_t s = (uint32_t)t * kSortChunk + i;
+                if (s < count) q.perm[atomicAdd(&cursor[persist_sort_bucket<F>(v, s)], 1u)] = s;
+            }
+            persist_signal(&q.hdr[5]);
+            continue;
+        }
+        t -= S;
+        if (t < G) {  // -------- H_msg + base_w of one group (longest first), then its layer-0 list
+            const uint32_t g = (uint32_t)t;
+            if (!persist_wait(&q.hdr[5], (uint32_t)S, err, q.wait_ns)) break;
+            const uint32_t s = sig_of(g);
             bool live = false;
-            if (s < v.count) {
+            if (s < count) {
                 const uint64_t smlen = v.smlen[s];
                 if (!verify_input_ok(v, s)) {  // too short, or a key index outside the table
                     v.status[s] = -1;
@@ -288,11 +395,13 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
         }
         t -= G;
         if (t < n_hpre) {  // -------- h_pre of one H node of one layer, for a group
-            const uint32_t g = (uint32_t)(t / ((unsigned long long)d * nh));
-            const uint32_t k = (uint32_t)(t - (unsigned long long)g * d * nh);
+            const uint32_t pos = (uint32_t)(t / ((unsigned long long)d * nh));
+            const uint32_t k = (uint32_t)(t - (unsigned long long)pos * d * nh);
+            const uint32_t g = group_at(pos);
             if (!persist_wait(&q.hdr[2], (uint32_t)K, err, q.wait_ns)) break;
-            const uint32_t s = g * 32 + lane;
-            if (s < v.count) verify_hpre_item<F>(v, ctx, (uint64_t)s * d * nh + k);
+            if (!persist_wait(&q.hdr[5], (uint32_t)S, err, q.wait_ns)) break;
+            const uint32_t s = sig_of(g);
+            if (s < count) verify_hpre_item<F>(v, ctx, (uint64_t)s * d * nh + k);
             persist_signal(&q.hpre_done[g]);
             continue;
         }
@@ -302,7 +411,20 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
         uint32_t leafidx;
         uint64_t tree;
         if (r < (unsigned long long)G * LEN) {  // -------- 32 chains of a group's list
-            const uint32_t c = (uint32_t)(r / G), g = (uint32_t)(r - (unsigned long long)c * G);
+            // bands: the groups of short H_msg (positions 0 .. GS-1), then the
+            // long ones; inside a band c-major, so longest chains go first
+            if (!persist_wait(&q.hdr[4], 1u, err, q.wait_ns)) break;
+            const uint32_t GL = min(G, (ld_relaxed(&q.hdr[6]) + 31) / 32), GS = G - GL;
+            uint32_t c, pos;
+            if (r < (unsigned long long)GS * LEN) {
+                c = (uint32_t)(r / GS);
+                pos = (uint32_t)(r - (unsigned long long)c * GS);
+            } else {
+                const unsigned long long r2 = r - (unsigned long long)GS * LEN;
+                c = (uint32_t)(r2 / GL);
+                pos = GS + (uint32_t)(r2 - (unsigned long long)c * GL);
+            }
+            const uint32_t g = group_at(pos);
             const uint32_t gl = g * d + layer;
             if (!persist_wait(&q.ready[gl], 1u, err, q.wait_ns)) break;
             if (layer == 0 && !persist_wait(&q.hdr[2], (uint32_t)K, err, q.wait_ns)) break;
@@ -336,7 +458,8 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
                 lev++;
             }
             const uint32_t items = (uint32_t)lt_items(LEN, lev);
-            const uint32_t g = (uint32_t)(r / items), p = (uint32_t)(r - (unsigned long long)g * items);
+            const uint32_t pos = (uint32_t)(r / items), p = (uint32_t)(r - (unsigned long long)pos * items);
+            const uint32_t g = group_at(pos);
             const uint32_t gl = g * d + layer;
             if (lev == 0) {
                 if (!persist_wait(&q.chains_done[gl], (uint32_t)LEN, err, q.wait_ns)) break;
@@ -344,8 +467,8 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
             } else if (!persist_wait(&q.lt_done[gl * 8 + lev - 1], (uint32_t)lt_items(LEN, lev - 1), err, q.wait_ns)) {
                 break;
             }
-            const uint32_t s = g * 32 + lane;
-            if (s < v.count && v.status[s] == 0) {
+            const uint32_t s = sig_of(g);
+            if (s < count && v.status[s] == 0) {
                 const int cin = lt_cnt(LEN, lev);
                 // levels alternate between the WOTS pk buffer and the half-size one
                 const bool even = (lev & 1) == 0;
@@ -370,10 +493,10 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
         }
         r -= (unsigned long long)G * LT;
         {  // -------- compute_root of a group, then the next layer's list or the verdict
-            const uint32_t g = (uint32_t)r, gl = g * d + layer;
+            const uint32_t g = group_at((uint32_t)r), gl = g * d + layer;
             if (!persist_wait(&q.lt_done[gl * 8 + LV - 1], 1u, err, q.wait_ns)) break;
-            const uint32_t s = g * 32 + lane;
-            const bool live = s < v.count && v.status[s] == 0;
+            const uint32_t s = sig_of(g);
+            const bool live = s < count && v.status[s] == 0;
             bool next_live = false;
             if (live) {
                 layer_addr<F>(v.idx[s], th, layer, leafidx, tree);

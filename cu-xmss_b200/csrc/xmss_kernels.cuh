@@ -167,6 +167,112 @@ __global__ void __launch_bounds__(128) k_keygen_chains(const TreeJob* __restrict
     }
 }
 
+// In-CTA subtrees: one thread per leaf, a CTA of 2^k threads builds a whole
+// subtree of height k (wots_pkgen + l_tree + the lowest k levels of
+// treehash, wots.c:117-131, xmss_commons.c:16-49, xmss_core.c:19-86).
+//
+// The thread computes its leaf's LEN chains in order (PRF_keygen + 15 F
+// each) and reduces them as they come: a stack in shared memory holds the
+// complete L-tree subtrees so far, whose sizes are the set bits of the
+// chains pushed (a binary counter), so chain ch merges with the stack top
+// once for every trailing one bit of ch.  After the last chain the odd
+// nodes are carried up exactly as l_tree carries them (a node alone at the
+// end of its level moves to the next level unhashed) and merged with the
+// remaining entries.  The hashes, their addresses and their order per node
+// are those of l_tree; nothing of the WOTS public key leaves the thread.
+// Then the 2^k leaves are reduced level by level in shared memory, and every
+// node of the subtree (levels 0..k) is written to the job's node array;
+// levels k+1..h follow as k_tree_level launches across CTAs.
+//
+// Grid: jobs x 2^(h-k) CTAs, numbered from cta0.  Dynamic shared memory:
+// subtree_smem<F>(2^k) bytes.
+__host__ __device__ constexpr int bit_width_c(int x) { return x ? 1 + bit_width_c(x >> 1) : 0; }
+
+template <class F>
+__host__ __device__ constexpr size_t subtree_smem(uint32_t threads)
+{
+    return (size_t)(bit_width_c(F::LEN) + 1) * threads * F::N;
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) k_keygen_subtree(const TreeJob* __restrict__ jobs, int h, int k, uint64_t cta0,
+                                                        const typename F::Ctx* __restrict__ ctx,
+                                                        uint8_t* __restrict__ nodes)
+{
+    constexpr int LEN = F::LEN, N = F::N, D = bit_width_c(F::LEN);
+    extern __shared__ __align__(16) uint8_t sh[];
+    const uint32_t B = blockDim.x;  // 2^k
+    const uint32_t t = threadIdx.x;
+    uint8_t* stk = sh + (size_t)t * N;            // entry e at stk + e * B * N
+    uint8_t* lvl = sh + (size_t)D * B * N;        // [B][N] nodes of the current level
+    const uint64_t cta = cta0 + blockIdx.x;
+    const int sub_bits = h - k;
+    const uint32_t j = (uint32_t)(cta >> sub_bits);
+    const uint64_t sub = cta & ((1ull << sub_bits) - 1);
+    const TreeJob job = jobs[j];
+    const uint32_t leaf = (uint32_t)((sub << k) + t);
+    const typename F::Ctx& c = ctx[job.key];
+    uint8_t* base = nodes + job.node_off;
+    uint32_t x[F::NW], a[8];
+    int sp = 0;
+#pragma unroll 1
+    for (uint32_t ch = 0; ch < (uint32_t)LEN; ch++) {
+        set_addr(a, job.layer, job.tree, ADDR_OTS, leaf, ch, 0);
+        run_chain<F>(x, c, a, 0, 15, true);
+        // node (level l, index ch >> l) merges while its index is odd
+#pragma unroll 1
+        for (uint32_t l = 0; (ch >> l) & 1; l++) {
+            uint32_t left[F::NW];
+            F::load(left, stk + (size_t)(--sp) * B * N);
+            set_addr(a, job.layer, job.tree, ADDR_LTREE, leaf, l, ch >> (l + 1));
+            F::thash_h(x, left, x, c, a);
+        }
+        F::store(stk + (size_t)(sp++) * B * N, x);
+    }
+    // The top entry (level L, index I) covers the last 2^L chains; the
+    // entries below it are the higher set bits R of LEN, lowest on top.  A
+    // node below the next entry's level is the last of its level with an
+    // even index: it moves up unhashed (l_tree's carry); at that level it is
+    // the right sibling of the entry, and they merge.
+    uint32_t L = __ffs(LEN) - 1, I = ((uint32_t)LEN >> L) - 1, R = (uint32_t)LEN & ((uint32_t)LEN - 1);
+    F::load(x, stk + (size_t)(--sp) * B * N);
+#pragma unroll 1
+    while (R) {
+        const uint32_t L2 = __ffs(R) - 1;
+        I >>= (L2 - L);
+        L = L2;
+        uint32_t left[F::NW];
+        F::load(left, stk + (size_t)(--sp) * B * N);
+        set_addr(a, job.layer, job.tree, ADDR_LTREE, leaf, L, I >> 1);
+        F::thash_h(x, left, x, c, a);
+        L++;
+        I >>= 1;
+        R &= R - 1;
+    }
+    // x is the leaf: level 0 of the subtree, then levels 1..k in shared memory
+    F::store(base + (level_offset(h, 0) + leaf) * N, x);
+    F::store(lvl + (size_t)t * N, x);
+    __syncthreads();
+#pragma unroll 1
+    for (int l = 0; l < k; l++) {
+        const uint32_t cnt = B >> (l + 1);
+        const uint32_t gi = (uint32_t)(sub << (k - l - 1)) + t;  // the parent's index on level l + 1
+        if (t < cnt) {
+            uint32_t le[F::NW], ri[F::NW];
+            F::load(le, lvl + (size_t)(2 * t) * N);
+            F::load(ri, lvl + (size_t)(2 * t + 1) * N);
+            set_addr(a, job.layer, job.tree, ADDR_HASHTREE, 0, (uint32_t)l, gi);
+            F::thash_h(x, le, ri, c, a);
+        }
+        __syncthreads();
+        if (t < cnt) {
+            F::store(lvl + (size_t)t * N, x);
+            F::store(base + (level_offset(h, l + 1) + gi) * N, x);
+        }
+        __syncthreads();
+    }
+}
+
 // One L-tree level (xmss_commons.c:16-49) for many leaf slots: item =
 // (slot, pair).  Pairs hash nodes 2p, 2p+1; an odd last node is carried up.
 // The final level (cnt_in == 2) writes the leaf to leaf_out + ref.out_off.

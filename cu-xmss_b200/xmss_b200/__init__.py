@@ -784,11 +784,53 @@ def autotune(oid: int, mt: bool, count: int = 4096):
     return best.as_dict(), json.loads(rep.value.decode())
 
 
-def save_tuning(path: str = TUNING_PATH, notes: dict | None = None) -> None:
-    """Writes the current shape of every family as a JSON table."""
+class TreeTuning(C.Structure):
+    """xmss_b200_tree_tuning (include/xmss_b200.h)."""
+
+    _fields_ = [("subtree_height", C.c_uint32), ("chains_per_warp", C.c_uint32), ("min_leaves", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+lib.xmss_b200_tree_tuning_get.argtypes = [C.c_uint32, C.c_int, C.POINTER(TreeTuning)]
+lib.xmss_b200_tree_tuning_set.argtypes = [C.c_uint32, C.c_int, C.POINTER(TreeTuning)]
+lib.xmss_b200_autotune_tree.argtypes = [C.c_uint32, C.c_int, C.POINTER(TreeTuning), C.c_char_p, C.c_size_t]
+
+
+def tree_tuning_get(oid: int, mt: bool) -> dict:
+    """How the subtrees of parameter set (oid, mt) are built."""
+    t = TreeTuning()
+    if lib.xmss_b200_tree_tuning_get(oid, int(mt), C.byref(t)):
+        raise ValueError(f"unknown parameter set ({oid:#x}, mt={mt})")
+    return t.as_dict()
+
+
+def tree_tuning_set(oid: int, mt: bool, subtree_height: int, min_leaves: int = 0) -> None:
+    t = TreeTuning(subtree_height=subtree_height, chains_per_warp=0, min_leaves=min_leaves)
+    if lib.xmss_b200_tree_tuning_set(oid, int(mt), C.byref(t)):
+        raise ValueError(f"tree_tuning_set: {last_error()}")
+
+
+def autotune_tree(oid: int, mt: bool):
+    """xmss_b200_autotune_tree: returns (chosen shape, report of every trial)."""
     import json
 
-    table = {"families": [{"func": f, "n": n, **tuning_get(f, n)} for f, n in FAMILIES]}
+    best = TreeTuning()
+    rep = C.create_string_buffer(1 << 14)
+    r = _check(lib.xmss_b200_autotune_tree(oid, int(mt), C.byref(best), rep, len(rep)), "autotune_tree")
+    if r:
+        raise ValueError(f"autotune_tree returned {r}: {last_error()}")
+    return best.as_dict(), json.loads(rep.value.decode())
+
+
+def save_tuning(path: str = TUNING_PATH, notes: dict | None = None, sets=()) -> None:
+    """Writes the current shape of every family, and the tree shape of the
+    parameter sets `sets` ((oid, mt) pairs), as a JSON table."""
+    import json
+
+    table = {"families": [{"func": f, "n": n, **tuning_get(f, n)} for f, n in FAMILIES],
+             "sets": [{"oid": oid, "mt": bool(mt), **tree_tuning_get(oid, mt)} for oid, mt in sets]}
     if notes:
         table["notes"] = notes
     with open(path, "w") as fh:
@@ -801,8 +843,11 @@ def load_tuning(path: str = TUNING_PATH) -> bool:
 
     if not os.path.exists(path):
         return False
-    for e in json.load(open(path))["families"]:
+    table = json.load(open(path))
+    for e in table["families"]:
         tuning_set(e["func"], e["n"], e)
+    for e in table.get("sets", []):
+        tree_tuning_set(e["oid"], e["mt"], e["subtree_height"], e["min_leaves"])
     return True
 
 

@@ -144,6 +144,42 @@ typedef struct {
 int xmss_b200_tuning_get(unsigned int func, unsigned int n, xmss_b200_tuning *out);
 int xmss_b200_tuning_set(unsigned int func, unsigned int n, const xmss_b200_tuning *t);
 
+/* How the subtrees of one parameter set (OID) are built, for keygen, sign
+ * and the server's subtree cache (treehash, xmss_core.c:19-86):
+ *   subtree_height 0    one thread per WOTS chain (chains_per_warp 32),
+ *                       then one launch per L-tree level and per Merkle
+ *                       level;
+ *   subtree_height 5-7  in-CTA subtrees: one thread per leaf
+ *                       (chains_per_warp 32 x len), whose chains are
+ *                       reduced into the L-tree as they finish, a CTA of
+ *                       2^k threads reducing its 2^k leaves to one node in
+ *                       shared memory; the levels above run across CTAs;
+ *   min_leaves          builds with fewer leaves in one call use the first
+ *                       form (the in-CTA form runs a leaf's chains one
+ *                       after the other, so small builds lack parallelism).
+ * chains_per_warp is reported by _get and ignored by _set.  Results do not
+ * depend on the shape.  Default: 0 (set by the autotuner or
+ * xmss_b200/tuning.json).  0 ok, -1 unknown OID or height out of range. */
+typedef struct {
+    uint32_t subtree_height;
+    uint32_t chains_per_warp;
+    uint64_t min_leaves;
+} xmss_b200_tree_tuning;
+
+int xmss_b200_tree_tuning_get(uint32_t oid, int mt, xmss_b200_tree_tuning *out);
+int xmss_b200_tree_tuning_set(uint32_t oid, int mt, const xmss_b200_tree_tuning *t);
+
+/* Tree autotuner for one parameter set: times keygen slices of 2^12, 2^15
+ * and 2^18 leaves (subtrees of the set's height, seeded keys) in the
+ * one-thread-per-chain form and as in-CTA subtrees of height 5, 6 and 7,
+ * checks that every form gives the same node arrays, and sets the set's
+ * shape: the in-CTA height that is fastest at 2^18 leaves if it beats the
+ * other form by 2 %, and min_leaves = the smallest slice at which it still
+ * does.  best gets the shape; report (if not NULL) a JSON text of every
+ * trial.  No reference counterpart (a launch-shape choice).  0 ok, -1
+ * unknown OID, -3 failure. */
+int xmss_b200_autotune_tree(uint32_t oid, int mt, xmss_b200_tree_tuning *best, char *report, size_t report_cap);
+
 /* Autotuner: times candidate shapes on a synthetic batch of this parameter
  * set (16 seeded keys, `count` signatures of messages log-uniform in
  * 32 B..4 KB, made by this library, and a 4,096-leaf keygen slice), one knob
@@ -378,7 +414,9 @@ int xmss_b200_sk_to_bds(int mt, const uint8_t *sk, uint8_t *bds_sk);
 /* Compression-rate probe (the roofline denominator): `blocks` x 128 threads
  * each run `iters` dependent SHA-256 compressions (kind 0), Keccak-f[1600]
  * permutations (kind 1) or SHA-512 compressions (kind 2) in registers, on
- * `stream`.  d_sink: blocks x 128
+ * `stream`; kinds 10 + m (m = 0..9) run SHA-256 in pipe mix m, and 20, 21
+ * and 23 mixes 0, 1 and 3 with one warp per block (latency of a lone warp).
+ * d_sink: blocks x 128
  * u32 of device memory (written almost never). */
 int xmss_b200_rate_probe(int kind, uint32_t blocks, uint32_t iters, uint32_t *d_sink, void *stream);
 

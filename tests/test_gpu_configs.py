@@ -40,6 +40,65 @@ def test_keygen_workload_keys_match_golden(xb, golden):
             assert sk[4:].tobytes() == bytes(ib) + seed[:2 * n] + want_pk[:n] + seed[2 * n:]
 
 
+@pytest.mark.parametrize("name", ["XMSS-SHA2_10_256", "XMSS-SHA2_10_192", "XMSS-SHA2_10_512", "XMSS-SHAKE_10_256",
+                                  "XMSS-SHAKE256_10_192", "XMSS-SHAKE_10_512", "XMSSMT-SHA2_20/4_256"])
+def test_in_cta_subtrees_match_oracle(xb, oracle, name):
+    """Subtrees built as in-CTA subtrees of height 5, 6 and 7 (one thread per
+    leaf, streaming L-tree, lower Merkle levels in shared memory; WOTS
+    lengths 51, 67 and 131) give the keys and signatures of the
+    one-thread-per-chain form and of the oracle."""
+    mt = name.startswith("XMSSMT")
+    oid = xb.xmssmt_str_to_oid(name) if mt else xb.xmss_str_to_oid(name)
+    p, po = xb.parse_oid(oid, mt), oracle.params(oid, mt)
+    rng = np.random.default_rng(zlib.crc32(name.encode()) + 1)
+    seeds = np.frombuffer(rng.bytes(3 * 3 * p.n), np.uint8).reshape(3, -1)
+    # the oracle's public key of the first seed (top-layer tree on all cores)
+    s0 = seeds[0].tobytes()
+    top = oracle.tree_nodes(po, s0[:p.n], s0[2 * p.n:], p.d - 1, 0, os.cpu_count() or 1)
+    saved = xb.tree_tuning_get(oid, mt)
+    try:
+        xb.tree_tuning_set(oid, mt, 0, 0)
+        want_pk, want_sk = xb.keypair_batch(oid, mt, seeds)
+        assert want_pk[0, 4:].tobytes() == top[-p.n:] + s0[2 * p.n:]
+        idx = int(rng.integers(0, (1 << p.full_height) - 1))
+        msg = rng.bytes(int(rng.integers(0, 3000)))
+        row = want_sk[:1].copy()
+        row[0, 4:4 + p.index_bytes] = np.frombuffer(idx.to_bytes(p.index_bytes, "big"), np.uint8)
+        ret, want_sm = xb.sign_batch(mt, row.copy(), [msg])
+        assert ret[0] == 0
+        for k in (5, 6, 7):
+            xb.tree_tuning_set(oid, mt, k, 0)
+            assert xb.tree_tuning_get(oid, mt)["chains_per_warp"] == 32 * p.wots_len
+            pk, sk = xb.keypair_batch(oid, mt, seeds)
+            assert (pk == want_pk).all() and (sk == want_sk).all(), (name, k)
+            ret, sm = xb.sign_batch(mt, row.copy(), [msg])
+            assert ret[0] == 0 and sm == want_sm, (name, k)
+        # the signature itself against the oracle
+        sk = row[0, 4:].tobytes()
+        ib, n, th = p.index_bytes, p.n, p.tree_height
+        trees = b"".join(oracle.tree_nodes(po, sk[ib:ib + n], sk[ib + 3 * n:ib + 4 * n], layer,
+                                           idx >> (th * (layer + 1)) if th * (layer + 1) < 64 else 0,
+                                           os.cpu_count() or 1) for layer in range(p.d))
+        assert oracle.sign(po, sk, msg, trees=trees)[2] == want_sm[0]
+    finally:
+        xb.tree_tuning_set(oid, mt, saved["subtree_height"], saved["min_leaves"])
+
+
+def test_in_cta_subtrees_keygen_workload_golden(xb, golden):
+    """The h = 16 and h = 20 golden keys again with the in-CTA form forced."""
+    doc = golden("keygen_config3.json")
+    for oid in (0x02, 0x03):
+        keys = [k for k in doc["keys"] if k["oid"] == oid][:2]
+        seeds = np.stack([np.frombuffer(bytes.fromhex(k["seed"]), np.uint8) for k in keys])
+        saved = xb.tree_tuning_get(oid, False)
+        try:
+            xb.tree_tuning_set(oid, False, 7, 0)
+            pks, _ = xb.keypair_batch(oid, False, seeds)
+        finally:
+            xb.tree_tuning_set(oid, False, saved["subtree_height"], saved["min_leaves"])
+        assert [pk[4:].tobytes().hex() for pk in pks] == [k["pk"] for k in keys]
+
+
 def test_bench_workload_same_bytes_from_gpu_and_oracle(xb):
     """bench.py's two arms build the verify workload independently: the GPU
     arm with this library, the reference arm with the CPU oracle.  Both
