@@ -73,6 +73,7 @@ void to_c(const xb::Tuning& t, xmss_b200_tuning* o)
     o->split_min = t.split_min;
     o->short_hmsg_blocks = t.short_hmsg_blocks;
     o->prep_split = t.prep_split;
+    o->persist_sort = t.persist_sort;
 }
 
 }  // namespace
@@ -87,7 +88,8 @@ extern "C" int xmss_b200_tuning_get(unsigned func, unsigned n, xmss_b200_tuning*
 extern "C" int xmss_b200_tuning_set(unsigned func, unsigned n, const xmss_b200_tuning* t)
 {
     if (!xb::family_ops(func, n) || !t || !block_ok(t->verify_chain_block) || !block_ok(t->keygen_chain_block) ||
-        !block_ok(t->level_block) || !t->split_min || !t->short_hmsg_blocks || t->prep_split > 1) {
+        !block_ok(t->level_block) || !t->split_min || !t->short_hmsg_blocks || t->prep_split > 1 ||
+        t->persist_sort > 1) {
         xb::set_last_error("xmss_b200_tuning_set: unknown family or shape out of range");
         return -1;
     }
@@ -99,6 +101,7 @@ extern "C" int xmss_b200_tuning_set(unsigned func, unsigned n, const xmss_b200_t
     d.split_min = t->split_min;
     d.short_hmsg_blocks = t->short_hmsg_blocks;
     d.prep_split = t->prep_split;
+    d.persist_sort = t->persist_sort;
     return 0;
 }
 
