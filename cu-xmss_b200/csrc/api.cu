@@ -281,6 +281,11 @@ namespace xb {
 // Lets other translation units of the library report through
 // xmss_b200_last_error.
 void set_last_error(const std::string& msg) { g_err = msg; }
+// The reference's index bookkeeping of one sign (sk without OID): 0 or -2.
+int sign_advance(const xmss_params& p, uint8_t* sk, uint64_t* idx, uint8_t* idx_bytes)
+{
+    return sk_advance(p, sk, idx, idx_bytes);
+}
 }  // namespace xb
 
 // ===========================================================================

@@ -318,7 +318,7 @@ void Engine::build_trees(const FamilyOps* ops, const TreeJob* d_jobs, uint32_t n
 }
 
 void Engine::keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_seeds,
-                     uint8_t* d_pk, uint8_t* d_sk, cudaStream_t st, Workspace& w)
+                     uint8_t* d_pk, uint8_t* d_sk, cudaStream_t st, Workspace& w, bool wait)
 {
     if (!count) return;
     const uint32_t n = p.n, th = p.tree_height;
@@ -335,7 +335,7 @@ void Engine::keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count,
                                           p.index_bytes, (uint32_t)p.sk_bytes, count, d_pk, d_sk);
     // the host job list is reused by the next call only after this one's
     // copy has been consumed
-    XB_CUDA(cudaStreamSynchronize(st));
+    if (wait) XB_CUDA(cudaStreamSynchronize(st));
 }
 
 // One launch sequence of verify (prep, then per layer: bucket, chains, L-tree,
@@ -503,10 +503,14 @@ void Engine::verify_persistent(const FamilyOps* ops, const xmss_params& p, uint3
     // counters, the H_msg length histogram and bucket cursors, and the
     // ready queue (8-byte entries); all of it starts at zero
     const size_t gl = (size_t)groups * d;
-    const size_t words = kPersistHdrWords + gl * 11 + groups + 2 * kSortBuckets;
+    const size_t words = kPersistHdrWords + gl * 11 + groups + 2 * kSortBuckets + kPersistSmSlots;
     const unsigned long long cap = persist_rq_cap(count, d, (int)len);
     const size_t rq_off = (8 + words * 4 + 7) & ~(size_t)7;
-    const size_t state_bytes = rq_off + cap * 8;
+    const unsigned long long cap_hi = persist_rqh_cap(count, d, (int)len);
+    // queue slots are 32-bit, the top two values mark "none"; groups are 24-bit in a task word
+    if (cap >= 0xFFFFFFF0ull || cap_hi >= 0xFFFFFFF0ull || groups >= (1u << 24))
+        throw CudaFailure("batch too large for one persistent launch");
+    const size_t state_bytes = rq_off + (cap + cap_hi) * 8;
     uint8_t* st8 = w.pstate.as<uint8_t>(state_bytes);
     uint32_t* u = (uint32_t*)(st8 + 8);
     PersistArgs q{};
@@ -518,8 +522,11 @@ void Engine::verify_persistent(const FamilyOps* ops, const xmss_params& p, uint3
     q.lt_done = q.gate + gl;
     q.hpre_done = q.lt_done + 8 * gl;
     q.sort = q.hpre_done + groups;
+    q.smctr = q.sort + 2 * kSortBuckets;
     q.rq = (unsigned long long*)(st8 + rq_off);
     q.rq_cap = cap;
+    q.rqh = q.rq + cap;
+    q.rqh_cap = cap_hi;
     q.perm = w.aux.as<uint32_t>(count);
     q.list = w.list.as<uint32_t>((size_t)groups * 32 * len);
     q.ctx = w.ctx.get((size_t)npk * ops->ctx_bytes);
@@ -528,6 +535,14 @@ void Engine::verify_persistent(const FamilyOps* ops, const xmss_params& p, uint3
     q.wait_ns = persist_wait_ns;
     q.short_blocks = tuning_for(ops->func, ops->n).short_hmsg_blocks;
     q.sorted = tuning_for(ops->func, ops->n).persist_sort;
+    // one H_msg CTA on each of the first SMs: four groups at a time per SM,
+    // at most a quarter of the SMs
+    q.hmsg_sms = 0;
+    if (tuning_for(ops->func, ops->n).persist_hmsg_sms) {
+        int sms = 0;
+        XB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+        q.hmsg_sms = std::min<uint32_t>((groups + 3) / 4, (uint32_t)std::max(1, sms / 4));
+    }
     XB_CUDA(cudaMemsetAsync(st8, 0, state_bytes, st));
     q.trace = nullptr;
     ptrace_last_ = nullptr;
@@ -570,7 +585,7 @@ void Engine::last_verify_work(unsigned long long out[3])
 
 void Engine::sign(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* h_sk,
                   const uint64_t* h_idx, uint8_t* d_sm, const uint64_t* d_sm_off, const uint64_t* d_mlen,
-                  cudaStream_t st, Workspace& w)
+                  cudaStream_t st, Workspace& w, bool wait)
 {
     if (!count) return;
     const uint32_t n = p.n, th = p.tree_height, d = p.d, ib = p.index_bytes;
@@ -653,7 +668,7 @@ void Engine::sign(const FamilyOps* ops, const xmss_params& p, uint32_t count, co
     mark(kChains, true, st);
     ops->sign_chains(g, ctx, st);
     mark(kChains, false, st);
-    XB_CUDA(cudaStreamSynchronize(st));  // staging buffers are reused by the next call
+    if (wait) XB_CUDA(cudaStreamSynchronize(st));  // staging buffers are reused by the next call
 }
 
 void Engine::core_hash(const FamilyOps* ops, uint32_t count, const uint8_t* d_in, const uint64_t* d_off,

@@ -176,8 +176,10 @@ class Engine {
     {
         keypair(ops, p, count, d_seeds, d_pk, d_sk, st, ws_);
     }
+    // wait false: returns without waiting for st (the caller keeps w's
+    // pinned job list unchanged until the work has run; graph capture).
     void keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_seeds, uint8_t* d_pk,
-                 uint8_t* d_sk, cudaStream_t st, Workspace& w);
+                 uint8_t* d_sk, cudaStream_t st, Workspace& w, bool wait = true);
 
     // Signing given per-request key material.  h_sk: count x sk_bytes (no
     // OID), already reflecting the reference's exhaustion handling; h_idx:
@@ -189,9 +191,10 @@ class Engine {
     {
         sign(ops, p, count, h_sk, h_idx, d_sm, d_sm_off, d_mlen, st, ws_);
     }
+    // wait as for keypair.
     void sign(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* h_sk,
               const uint64_t* h_idx, uint8_t* d_sm, const uint64_t* d_sm_off, const uint64_t* d_mlen,
-              cudaStream_t st, Workspace& w);
+              cudaStream_t st, Workspace& w, bool wait = true);
 
     void core_hash(const FamilyOps* ops, uint32_t count, const uint8_t* d_in, const uint64_t* d_off,
                    const uint64_t* d_len, uint8_t* d_out, cudaStream_t st);

@@ -71,6 +71,10 @@ enum : uint32_t {
     kPhFinished = 7,   // groups whose last layer is done
     kPhHead = 8,       // ready queue: next entry to take
     kPhTail = 9,       // ready queue: entries reserved
+    kPhHmsgTicket = 10,  // next hmsg task
+    kPhHmsgDone = 11,  // hmsg tasks done
+    kPhHeadHi = 12,    // high-priority queue: next entry to take
+    kPhTailHi = 13,    // high-priority queue: entries reserved
     kPersistHdrWords = 16
 };
 
@@ -78,7 +82,8 @@ enum : uint32_t {
 struct PersistArgs {
     unsigned long long* ticket;  // next static ticket
     uint32_t* hdr;               // [kPersistHdrWords], see above
-    unsigned long long* rq;      // ready queue [rq_cap]: task word | kReady once written
+    unsigned long long* rq;      // ready queue of chain tasks [rq_cap]: task word | kReady once written
+    unsigned long long* rqh;     // high-priority ready queue of L-tree and root tasks [rqh_cap]
     uint32_t* ntot;              // [G*d] chain entries in the list of (group, layer)
     uint32_t* chains_done;       // [G*d] chain tasks finished
     uint32_t* gate;              // [G*d] inputs of L-tree level 0 complete: chains (1) and h_pre (1)
@@ -87,13 +92,16 @@ struct PersistArgs {
     uint32_t* list;              // [G][32*LEN] chain items (s*LEN + chain) of the group's current layer
     uint32_t* perm;              // [count] signatures in group order
     uint32_t* sort;              // [2 * kSortBuckets] histogram, then bucket cursors
+    uint32_t* smctr;             // [kPersistSmSlots] CTAs arrived per SM
     void* ctx;                   // [npk] F::Ctx, written by the ctx tasks
     unsigned long long wait_ns;  // bound of one wait (%globaltimer ns)
-    unsigned long long rq_cap;   // ready-queue entries
+    unsigned long long rq_cap;   // chain-queue entries
+    unsigned long long rqh_cap;  // high-priority-queue entries
     uint32_t npk;
     uint32_t groups;
     uint32_t short_blocks;       // hash blocks of H_msg that count as long (hdr[kPhLong])
     uint32_t sorted;             // 1: groups sorted by H_msg length; 0: batch order
+    uint32_t hmsg_sms;           // SMs 0 .. hmsg_sms-1 start with one CTA of hmsg tasks (0: none)
     unsigned long long* trace;   // optional [kTrKinds][4]: ~first start, last end, busy ns, tasks
 };
 
@@ -108,6 +116,9 @@ enum : uint32_t {
 // produced by tasks already running, so a legitimate wait lasts at most about
 // one H_msg: 8 s is a message of several hundred MB.
 constexpr unsigned long long kPersistWaitNs = 8000000000ull;
+
+// SMs whose arrivals are counted (H_msg CTAs go to SMs below hmsg_sms).
+constexpr uint32_t kPersistSmSlots = 256;
 
 // L-tree shape (xmss_commons.c:16-49): level l reduces cnt(l) nodes into
 // items(l) = ceil(cnt/2) (the odd node is carried up); its hashed pairs are
@@ -146,10 +157,15 @@ __host__ __device__ constexpr int lt_items_total(int len)
 static_assert(lt_levels(131) <= 8 && lt_levels(67) == 7 && lt_items_total(67) == 71, "L-tree shape");
 
 // Ready-queue entries a launch can push at most: per (group, layer) at most
-// LEN chain tasks, every L-tree task and one root task.
+// LEN chain tasks (chain queue), and every L-tree task and one root task
+// (high-priority queue).
 __host__ __device__ inline unsigned long long persist_rq_cap(uint32_t count, uint32_t d, int len)
 {
-    return (unsigned long long)((count + 31) / 32) * d * (len + lt_items_total(len) + 1);
+    return (unsigned long long)((count + 31) / 32) * d * len;
+}
+__host__ __device__ inline unsigned long long persist_rqh_cap(uint32_t count, uint32_t d, int len)
+{
+    return (unsigned long long)((count + 31) / 32) * d * (lt_items_total(len) + 1);
 }
 
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p)
@@ -254,54 +270,101 @@ __device__ __forceinline__ unsigned long long task_word(uint32_t kind, uint32_t 
            ((unsigned long long)g << 24) | i;
 }
 
-// Pushes n tasks (index 0 .. n-1 of `base`) onto the ready queue (whole warp).
-__device__ __forceinline__ void persist_push(const PersistArgs& q, unsigned long long base, uint32_t n)
+// Pushes n tasks (index 0 .. n-1 of `base`) onto the chain queue or, with
+// hi, the high-priority queue (whole warp).
+__device__ __forceinline__ void persist_push(const PersistArgs& q, unsigned long long base, uint32_t n, bool hi)
 {
     if (!n) return;
     uint32_t first = 0;
-    if ((threadIdx.x & 31) == 0) first = atomicAdd(&q.hdr[kPhTail], n);
+    if ((threadIdx.x & 31) == 0) first = atomicAdd(&q.hdr[hi ? kPhTailHi : kPhTail], n);
     first = __shfl_sync(0xffffffffu, first, 0);
+    unsigned long long* qe = hi ? q.rqh : q.rq;
     for (uint32_t i = threadIdx.x & 31; i < n; i += 32) {
-        unsigned long long* e = q.rq + first + i;
+        unsigned long long* e = qe + first + i;
         asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(e), "l"((base + i) | kReady) : "memory");
     }
 }
 
-// Claims the next ready-queue slot for the warp (one atomic add, no retry)
-// and waits until its entry is written, the launch has finished (`groups`
-// groups done: no more entries will come) or failed, or the wait bound runs
-// out (the error flag is then set).  Returns the task word, or 0 when the
-// warp should leave.  Whole warp; lane 0 claims and polls its own slot.
-__device__ __forceinline__ unsigned long long persist_take(const PersistArgs& q, uint32_t groups)
+// Every lane acquires a taken entry, so each one's loads see what the task's
+// producers wrote before publishing it.
+__device__ __forceinline__ void persist_acquire_entry(const unsigned long long* e)
+{
+    (void)ld_acquire64(e);
+}
+
+// Slot values of a warp: none claimed, and (high-priority queue) every slot
+// already claimed by some warp.
+constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+constexpr uint32_t kHiDone = 0xFFFFFFFEu;
+
+// Claims a high-priority slot when the queue shows an entry nobody has
+// claimed yet: one atomic add, never a retry loop (a compare-and-swap head
+// serialised the claims of thousands of polling warps).  A warp that raced
+// past the tail owns a slot whose entry comes later; every slot below
+// rqh_cap gets exactly one entry, since each (group, layer) pushes all of its
+// L-tree tasks and one root.  Whole warp.
+__device__ __forceinline__ uint32_t persist_claim_hi(const PersistArgs& q)
+{
+    uint32_t slot = kNoSlot;
+    if ((threadIdx.x & 31) == 0) {
+        const uint32_t h = ld_relaxed(&q.hdr[kPhHeadHi]);
+        if (h >= q.rqh_cap) {
+            slot = kHiDone;
+        } else if (h < ld_relaxed(&q.hdr[kPhTailHi])) {
+            slot = atomicAdd(&q.hdr[kPhHeadHi], 1u);
+            if (slot >= q.rqh_cap) slot = kHiDone;
+        }
+    }
+    return __shfl_sync(0xffffffffu, slot, 0);
+}
+
+// Claims the next chain-queue slot (one atomic add, no retry; the warp then
+// owns it until its entry arrives).  Whole warp.
+__device__ __forceinline__ uint32_t persist_claim_lo(const PersistArgs& q)
+{
+    uint32_t slot = 0;
+    if ((threadIdx.x & 31) == 0) slot = atomicAdd(&q.hdr[kPhHead], 1u);
+    return __shfl_sync(0xffffffffu, slot, 0);
+}
+
+// Polls the warp's claimed slots a few times, the high-priority one first
+// (relaxed loads with growing sleeps: an acquire per poll would order the
+// SM's L1 against the GPU every time, evicting what the working warps read).
+// Returns the task word and clears the slot it came from, or 0 when neither
+// entry has arrived yet.  Whole warp.
+__device__ __forceinline__ unsigned long long persist_poll(const PersistArgs& q, uint32_t& hi_slot,
+                                                           uint32_t& lo_slot, int polls)
 {
     unsigned long long w = 0;
-    uint32_t slot = 0;
+    uint32_t from = 0;  // 1: high-priority slot, 2: chain slot
     if ((threadIdx.x & 31) == 0) {
-        slot = atomicAdd(&q.hdr[kPhHead], 1u);
-        const unsigned long long t0 = global_ns();
-        unsigned ns = 64;
-        // relaxed polls: an acquire per poll would order the SM's L1 against
-        // the GPU every time, evicting what the working warps read
-        for (uint32_t polls = 0;; polls++) {
-            if (slot < q.rq_cap && ((w = ld_relaxed64(q.rq + slot)) & kReady)) break;
-            w = 0;
-            if ((polls & 7) == 7) {
-                if (*(volatile uint32_t*)&q.hdr[kPhErr] || ld_relaxed(&q.hdr[kPhFinished]) >= groups) break;
-                if (global_ns() - t0 > q.wait_ns) {
-                    atomicExch(&q.hdr[kPhErr], 1u);
-                    break;
-                }
+        // a chain slot beyond the queue never gets an entry: the warp only
+        // sleeps (and comes back for high-priority tasks, or to leave)
+        unsigned ns = 128;
+        for (int i = 0; i < polls; i++) {
+            if (hi_slot < kHiDone && ((w = ld_relaxed64(q.rqh + hi_slot)) & kReady)) {
+                from = 1;
+                break;
             }
-            __nanosleep(ns);
-            if (ns < 2048) ns *= 2;
+            if (lo_slot != kNoSlot && lo_slot < q.rq_cap && ((w = ld_relaxed64(q.rq + lo_slot)) & kReady)) {
+                from = 2;
+                break;
+            }
+            w = 0;
+            if (i + 1 < polls) {
+                __nanosleep(ns);
+                ns *= 2;
+            }
         }
     }
     w = __shfl_sync(0xffffffffu, w, 0);
-    if (w) {
-        // every lane acquires the entry, so each one's loads see what the
-        // task's producers wrote before publishing it
-        slot = __shfl_sync(0xffffffffu, slot, 0);
-        (void)ld_acquire64(q.rq + slot);
+    from = __shfl_sync(0xffffffffu, from, 0);
+    if (from == 1) {
+        persist_acquire_entry(q.rqh + hi_slot);
+        hi_slot = kNoSlot;
+    } else if (from == 2) {
+        persist_acquire_entry(q.rq + lo_slot);
+        lo_slot = kNoSlot;
     }
     return w;
 }
@@ -392,13 +455,15 @@ __host__ __device__ inline unsigned long long persist_static_tasks(uint32_t coun
 {
     const unsigned long long G = (count + 31) / 32, K = (npk + 31) / 32, S = (count + kSortChunk - 1) / kSortChunk;
     const unsigned long long nh = (unsigned long long)len - 1 + th;
-    return 2 * S + 1 + K + G + G * d * nh;
+    return 2 * S + 1 + K + G * d * nh;
 }
 
 // F runs every task except the chains, which run FT (same family, another
-// pipe mix; the key context is shared).
-template <class F, class FT>
-__global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(VerifyArgs v, PersistArgs q)
+// pipe mix; the key context is shared).  EXTRA CTAs per SM beyond
+// persist_min_ctas trade spills for occupancy (a tuning knob,
+// Tuning::persist_extra_ctas).
+template <class F, class FT, int EXTRA = 0>
+__global__ void __launch_bounds__(128, persist_min_ctas<F>() + EXTRA) k_verify_persist(VerifyArgs v, PersistArgs q)
 {
     using Ctx = typename F::Ctx;
     using HPre = typename F::HPre;
@@ -429,7 +494,7 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
     auto push_chains = [&](uint32_t g, uint32_t layer, uint32_t ntot) -> bool {
         const uint32_t nct = (ntot + 31) / 32;
         if (nct) {
-            persist_push(q, task_word(kTaskChain, layer, 0, g, 0), nct);
+            persist_push(q, task_word(kTaskChain, layer, 0, g, 0), nct, false);
             return false;
         }
         return true;  // caller runs the gate
@@ -442,7 +507,7 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
         second = __shfl_sync(0xffffffffu, second, 0);
         if (second) {
             __threadfence();
-            persist_push(q, task_word(kTaskLtree, layer, 0, g, 0), (uint32_t)lt_items(LEN, 0));
+            persist_push(q, task_word(kTaskLtree, layer, 0, g, 0), (uint32_t)lt_items(LEN, 0), true);
         }
     };
 
@@ -468,8 +533,89 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
         }
     };
 
-    bool static_left = true;
-    for (;;) {
+    // H_msg + base_w of group g (longest first when sorted), then its
+    // layer-0 chain tasks; false when a wait ran out
+    auto run_hmsg = [&](uint32_t g) -> bool {
+        if (!persist_wait(&q.hdr[kPhScatter], (uint32_t)S, err, q.wait_ns)) return false;
+        // the chain tasks read the key contexts
+        if (!persist_wait(&q.hdr[kPhCtx], (uint32_t)K, err, q.wait_ns)) return false;
+        const uint32_t s = sig_of(g);
+        bool live = false;
+        if (s < count) {
+            const uint64_t smlen = v.smlen[s];
+            if (!verify_input_ok(v, s)) {  // too short, or a key index outside the table
+                v.status[s] = -1;
+            } else {
+                const uint8_t* sm = v.sm + v.sm_off[s];
+                const uint64_t idx = bytes_be(sm, (int)v.index_bytes);
+                uint32_t mh[F::NW];
+                if constexpr (std::is_same<typename F::Ctx, Sha256N32Ctx>::value) {
+                    // the register-lean form keeps the kernel at the chains' register count
+                    hmsg_sha256_n32_lean(mh, sm + v.index_bytes, v.key_root + (uint64_t)v.key[s] * v.key_stride,
+                                         idx, sm + v.sig_bytes, smlen - v.sig_bytes);
+                } else {
+                    uint32_t R[F::NW], root[F::NW];
+                    F::load(R, sm + v.index_bytes);
+                    F::load(root, v.key_root + (uint64_t)v.key[s] * v.key_stride);
+                    hmsg<F>(mh, R, root, idx, sm + v.sig_bytes, smlen - v.sig_bytes);
+                }
+                F::store(v.node + (uint64_t)s * F::N, mh);
+                chain_lengths<F>(v.lens + (uint64_t)s * F::LEN, mh);
+                v.idx[s] = idx;
+                v.status[s] = 0;
+                live = true;
+                if (v.work) {
+                    atomicAdd(&v.work[0], hmsg_blocks<F>(smlen - v.sig_bytes));
+                    atomicAdd(&v.work[2], (unsigned long long)nh * d);
+                }
+            }
+        }
+        const uint32_t ntot = persist_bucket<F>(v, q, g, 0, live, s, cnt);
+        if (push_chains(g, 0, ntot)) gate(g, 0);
+        persist_signal(&q.hdr[kPhHmsgDone]);
+        return true;
+    };
+
+    // Role of this CTA: on the first hmsg_sms SMs the first CTA to arrive runs
+    // hmsg tasks first (one warp per SM sub-partition, so each serial H_msg
+    // gets most of its sub-partition's issue slots) and the other CTAs there
+    // wait until every hmsg task is done; all others start with the static
+    // tickets.  Every warp also takes hmsg tickets once its static tickets run
+    // out, so the launch never depends on where its CTAs land.
+    __shared__ uint32_t sh_role;
+    if (threadIdx.x == 0) {
+        uint32_t role = 0;
+        if (q.hmsg_sms) {
+            uint32_t smid;
+            asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+            if (smid < q.hmsg_sms && smid < kPersistSmSlots) role = atomicAdd(&q.smctr[smid], 1u) == 0 ? 1 : 2;
+        }
+        sh_role = role;
+    }
+    __syncthreads();
+    bool run = true;
+    if (sh_role == 1) {
+        for (;;) {
+            unsigned long long t = 0;
+            if (lane == 0) t = atomicAdd(&q.hdr[kPhHmsgTicket], 1u);
+            t = __shfl_sync(0xffffffffu, t, 0);
+            if (t >= G) break;
+            tr_begin(kTrHmsg);
+            if (!run_hmsg((uint32_t)t)) {
+                run = false;
+                break;
+            }
+            tr_end();
+        }
+    } else if (sh_role == 2) {
+        run = persist_wait(&q.hdr[kPhHmsgDone], G, err, q.wait_ns);
+    }
+
+    bool static_left = true, hmsg_left = true;
+    uint32_t lo_slot = kNoSlot;  // chain-queue slot this warp has claimed
+    uint32_t hi_slot = kNoSlot;  // high-priority slot this warp has claimed (kHiDone: none left)
+    unsigned long long idle_since = 0;
+    for (; run;) {
         tr_end();
         // decisions are made by lane 0 and broadcast: the warp stays converged
         if (__shfl_sync(0xffffffffu, *(volatile uint32_t*)err, 0)) break;
@@ -483,7 +629,7 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
                 continue;
             }
             tr_begin(t < S ? kTrCount : t < S + K ? kTrCtx : t < S + K + 1 ? kTrPrefix
-                     : t < 2 * S + K + 1 ? kTrScatter : t < 2 * S + K + 1 + G ? kTrHmsg : kTrHpre);
+                     : t < 2 * S + K + 1 ? kTrScatter : kTrHpre);
             if (t < S) {  // -------- count: H_msg length histogram of 1,024 signatures
                 for (uint32_t i = lane; q.sorted && i < kSortChunk; i += 32) {
                     const uint32_t s = (uint32_t)t * kSortChunk + i;
@@ -545,40 +691,6 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
                 continue;
             }
             t -= S;
-            if (t < G) {  // -------- H_msg + base_w of one group (longest first), then its layer-0 chains
-                const uint32_t g = (uint32_t)t;
-                if (!persist_wait(&q.hdr[kPhScatter], (uint32_t)S, err, q.wait_ns)) break;
-                // the chain tasks read the key contexts
-                if (!persist_wait(&q.hdr[kPhCtx], (uint32_t)K, err, q.wait_ns)) break;
-                const uint32_t s = sig_of(g);
-                bool live = false;
-                if (s < count) {
-                    const uint64_t smlen = v.smlen[s];
-                    if (!verify_input_ok(v, s)) {  // too short, or a key index outside the table
-                        v.status[s] = -1;
-                    } else {
-                        const uint8_t* sm = v.sm + v.sm_off[s];
-                        const uint64_t idx = bytes_be(sm, (int)v.index_bytes);
-                        uint32_t R[F::NW], root[F::NW], mh[F::NW];
-                        F::load(R, sm + v.index_bytes);
-                        F::load(root, v.key_root + (uint64_t)v.key[s] * v.key_stride);
-                        hmsg<F>(mh, R, root, idx, sm + v.sig_bytes, smlen - v.sig_bytes);
-                        F::store(v.node + (uint64_t)s * F::N, mh);
-                        chain_lengths<F>(v.lens + (uint64_t)s * F::LEN, mh);
-                        v.idx[s] = idx;
-                        v.status[s] = 0;
-                        live = true;
-                        if (v.work) {
-                            atomicAdd(&v.work[0], hmsg_blocks<F>(smlen - v.sig_bytes));
-                            atomicAdd(&v.work[2], (unsigned long long)nh * d);
-                        }
-                    }
-                }
-                const uint32_t ntot = persist_bucket<F>(v, q, g, 0, live, s, cnt);
-                if (push_chains(g, 0, ntot)) gate(g, 0);
-                continue;
-            }
-            t -= G;
             if (t < n_hpre) {  // -------- h_pre of one H node of one layer, for a group
                 const uint32_t pos = (uint32_t)(t / ((unsigned long long)d * nh));
                 const uint32_t k = (uint32_t)(t - (unsigned long long)pos * d * nh);
@@ -594,10 +706,47 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
             continue;  // not reached: t < total_static
         }
         // ---------------- then the next ready slot (or leave) ----------------
-        tr_begin(kTrIdle);
-        const unsigned long long w = persist_take(q, G);
-        tr_end();
-        if (!w) break;
+        // ---------------- high-priority tasks first: L-tree levels and roots ----------------
+        if (hi_slot == kNoSlot) hi_slot = persist_claim_hi(q);
+        uint32_t no_lo = kNoSlot;
+        unsigned long long w = hi_slot < kHiDone ? persist_poll(q, hi_slot, no_lo, 1) : 0;
+        if (!w) {
+            // ---------------- then hmsg tickets no H_msg CTA took ----------------
+            if (hmsg_left) {
+                unsigned long long t = 0;
+                if (lane == 0) t = atomicAdd(&q.hdr[kPhHmsgTicket], 1u);
+                t = __shfl_sync(0xffffffffu, t, 0);
+                if (t < G) {
+                    tr_begin(kTrHmsg);
+                    if (!run_hmsg((uint32_t)t)) break;
+                    continue;
+                }
+                hmsg_left = false;
+            }
+            // ---------------- then the warp's chain slot ----------------
+            if (lo_slot == kNoSlot) lo_slot = persist_claim_lo(q);
+            tr_begin(kTrIdle);
+            w = persist_poll(q, hi_slot, lo_slot, 6);
+            tr_end();
+            if (!w) {
+                // nothing yet: leave when every group is done, fail when idle too long
+                uint32_t stop = 0;
+                if (lane == 0) {
+                    const unsigned long long now = global_ns();
+                    if (ld_relaxed(&q.hdr[kPhFinished]) >= G) {
+                        stop = 1;
+                    } else if (!idle_since) {
+                        idle_since = now;
+                    } else if (now - idle_since > q.wait_ns) {
+                        atomicExch(err, 1u);
+                        stop = 1;
+                    }
+                }
+                if (__shfl_sync(0xffffffffu, stop, 0)) break;
+                continue;
+            }
+        }
+        idle_since = 0;
         {
             const uint32_t kind = (uint32_t)(w >> 60) & 7, layer = (uint32_t)(w >> 52) & 0xFF;
             tr_begin(kind == kTaskChain ? kTrChain : kind == kTaskLtree ? kTrLtree : kTrRoot);
@@ -658,9 +807,10 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
                 }
                 if (persist_finish(&q.lt_done[gl * 8 + lev], (uint32_t)lt_items(LEN, (int)lev))) {
                     if ((int)lev + 1 < LV)
-                        persist_push(q, task_word(kTaskLtree, layer, lev + 1, g, 0), (uint32_t)lt_items(LEN, lev + 1));
+                        persist_push(q, task_word(kTaskLtree, layer, lev + 1, g, 0), (uint32_t)lt_items(LEN, lev + 1),
+                                     true);
                     else
-                        persist_push(q, task_word(kTaskRoot, layer, 0, g, 0), 1);
+                        persist_push(q, task_word(kTaskRoot, layer, 0, g, 0), 1, true);
                 }
                 continue;
             }

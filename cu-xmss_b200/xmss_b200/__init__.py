@@ -121,7 +121,8 @@ class Tuning(C.Structure):
     """xmss_b200_tuning (include/xmss_b200.h)."""
 
     _fields_ = [(k, C.c_uint32) for k in ("verify_chain_block", "keygen_chain_block", "level_block", "split_min",
-                                          "short_hmsg_blocks", "prep_split", "persist_sort")]
+                                          "short_hmsg_blocks", "prep_split", "persist_sort",
+                                          "persist_extra_ctas", "persist_hmsg_sms")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -756,6 +757,69 @@ class VerifyGraph:
     def close(self) -> None:
         if self._h:
             lib.xmss_b200_verify_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+KEYGEN, SIGN, VERIFY = 1, 2, 3
+
+
+class BatchGroup(C.Structure):
+    """xmss_b200_batch_group: one kind and one parameter set of a mixed batch
+    (d_ fields are device pointers as ints; sk / ret host buffers)."""
+    _fields_ = [("kind", C.c_int), ("oid", C.c_uint32), ("mt", C.c_int), ("count", C.c_uint32),
+                ("d_seeds", C.c_void_p), ("d_pk", C.c_void_p), ("d_sk", C.c_void_p), ("sk", C.c_void_p),
+                ("ret", C.c_void_p), ("d_sm", C.c_void_p), ("d_sm_off", C.c_void_p), ("d_len", C.c_void_p),
+                ("npk", C.c_uint32), ("d_pk_index", C.c_void_p), ("d_status", C.c_void_p)]
+
+
+lib.xmss_b200_batch_create.argtypes = [C.POINTER(BatchGroup), C.c_uint32, C.POINTER(C.c_void_p)]
+lib.xmss_b200_batch_launch.argtypes = [C.c_void_p, C.c_void_p]
+lib.xmss_b200_batch_destroy.argtypes = [C.c_void_p]
+lib.xmss_b200_batch_destroy.restype = None
+
+
+class Batch:
+    """xmss_b200_batch_*: keygen / sign / verify groups of any parameter sets
+    captured in one CUDA graph.  groups: dicts of BatchGroup fields; a sign
+    group's "sk" is a writable uint8 numpy array (count x (4 + sk_bytes)),
+    advanced in place by create, and its codes land in self.ret[i]."""
+
+    def __init__(self, groups: Sequence[dict]):
+        arr = (BatchGroup * len(groups))()
+        self._keep = []
+        self.ret = []
+        for i, g in enumerate(groups):
+            g = dict(g)
+            ret = None
+            if g.get("kind") == SIGN:
+                sk = g.pop("sk")
+                assert sk.dtype == np.uint8 and sk.flags.c_contiguous and sk.flags.writeable
+                ret = np.zeros(int(g["count"]), np.int32)
+                g["sk"] = sk.ctypes.data
+                g["ret"] = ret.ctypes.data
+                self._keep += [sk, ret]
+            self.ret.append(ret)
+            for k, v in g.items():
+                setattr(arr[i], k, v)
+        h = C.c_void_p()
+        r = _check(lib.xmss_b200_batch_create(arr, len(groups), C.byref(h)), "batch_create")
+        if r:
+            raise ValueError(f"batch_create returned {r}: {last_error()}")
+        self._h = h
+
+    def launch(self, stream: int = 0) -> int:
+        """0, or -2 when a batch with sign groups is launched again."""
+        return _check(lib.xmss_b200_batch_launch(self._h, stream), "batch_launch")
+
+    def close(self) -> None:
+        if self._h:
+            lib.xmss_b200_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -121,6 +121,64 @@ int xmss_b200_verify_graph_create(uint32_t oid, int mt, uint32_t count, const ui
 int xmss_b200_verify_graph_launch(xmss_b200_verify_graph *g, void *stream);
 void xmss_b200_verify_graph_destroy(xmss_b200_verify_graph *g);
 
+/* Mixed batches: keygen, sign and verify groups of any parameter sets (OIDs,
+ * XMSS and XMSS^MT, every hash family) in ONE CUDA graph.  Each group is
+ * `count` items of one kind and one parameter set; its launch sequence (the
+ * one of xmss_b200_keypair_device / xmss_b200_sign_batch /
+ * xmss_b200_sign_open_device) is captured on a stream of its own, forked
+ * from and joined back into the launch stream, so the groups run
+ * concurrently and the whole batch is a single cudaGraphLaunch.  Every
+ * result is byte-identical to the per-kind calls (and to the reference's
+ * xmssmt_core_seed_keypair / xmss[mt]_sign / xmss[mt]_sign_open per item).
+ *
+ * Fields per kind (all d_ pointers on the device, read or written at each
+ * launch; host pointers only at create):
+ *   XMSS_B200_KEYGEN  d_seeds (count x 3n) -> d_pk (count x 2n, root ||
+ *                     PUB_SEED) and d_sk (count x sk_bytes), no OID prefix.
+ *   XMSS_B200_SIGN    sk: HOST, count x (4 + sk_bytes), OID-prefixed keys as
+ *                     xmss[mt]_keypair writes them (rows may repeat a key:
+ *                     its requests take consecutive indices); create does
+ *                     the reference's index bookkeeping (xmss_core.c:
+ *                     209-239) on them, so on return they are the keys to
+ *                     persist, and sets ret[i] (HOST) to 0 or -2 (exhausted:
+ *                     that item is not signed).  d_sm + d_sm_off[i] holds
+ *                     message i at offset sig_bytes (d_len[i] bytes); launch
+ *                     writes the signature before it.
+ *   XMSS_B200_VERIFY  d_sm / d_sm_off / d_len (signed-message lengths) /
+ *                     d_pk (npk x 2n) / npk / d_pk_index -> d_status, as in
+ *                     xmss_b200_sign_open_device.
+ * Each signing index is used once: a batch holding sign groups launches at
+ * most once (a second launch returns -2 and runs nothing); create signs
+ * nothing that leaves the library (its sizing run writes into scratch).
+ * Batches of keygen and verify groups may be relaunched after refilling
+ * their buffers; launches of one batch must not overlap.  create: 0 ok, -1
+ * bad group, -3 GPU failure; destroy waits for the device. */
+enum { XMSS_B200_KEYGEN = 1, XMSS_B200_SIGN = 2, XMSS_B200_VERIFY = 3 };
+
+typedef struct {
+    int kind;                    /* XMSS_B200_KEYGEN / _SIGN / _VERIFY */
+    uint32_t oid;                /* parameter set */
+    int mt;                      /* 1: XMSS^MT OID */
+    uint32_t count;              /* items */
+    const uint8_t *d_seeds;      /* keygen */
+    uint8_t *d_pk;               /* keygen: out; verify: in */
+    uint8_t *d_sk;               /* keygen */
+    uint8_t *sk;                 /* sign: host keys, advanced by create */
+    int *ret;                    /* sign: host per-item codes, set by create */
+    uint8_t *d_sm;               /* sign: out; verify: in */
+    const uint64_t *d_sm_off;    /* sign, verify */
+    const uint64_t *d_len;       /* sign: message lengths; verify: signed-message lengths */
+    uint32_t npk;                /* verify */
+    const uint32_t *d_pk_index;  /* verify */
+    int *d_status;               /* verify */
+} xmss_b200_batch_group;
+
+typedef struct xmss_b200_batch xmss_b200_batch;
+
+int xmss_b200_batch_create(const xmss_b200_batch_group *groups, uint32_t ngroups, xmss_b200_batch **out);
+int xmss_b200_batch_launch(xmss_b200_batch *b, void *stream);
+void xmss_b200_batch_destroy(xmss_b200_batch *b);
+
 /* Launch shapes of one hash family (func, n): CTA sizes (32, 64 or 128
  * threads) of the verify chain kernel, of the keygen / sign chain kernels
  * and of the L-tree / Merkle-level kernels, and the split of large verify
@@ -133,9 +191,15 @@ void xmss_b200_verify_graph_destroy(xmss_b200_verify_graph *g);
  * signatures by H_msg length (a device counting sort at the head of its
  * queue; longest H_msg first, the other tasks shortest first, chains in
  * two bands split at short_hmsg_blocks); 0 keeps them in batch order.
- * Results do not depend on any of them.  Defaults: 128, 128, 128, 1024, 16,
- * 1, 0.  Set them while no call of that family runs (they are read at each
- * launch). */
+ * persist_extra_ctas (0, 1, 2) raises the persistent verify's resident
+ * CTAs per SM above its spill-free count, trading register spills for
+ * occupancy.  persist_hmsg_sms = 1 starts the persistent verify with one
+ * CTA of H_msg tasks on each of the first SMs (four groups at a time per
+ * SM, one per sub-partition, at most a quarter of the SMs) while the other
+ * CTAs there wait for H_msg to finish, so the serial H_msg chains run
+ * nearly alone.  Results do not depend on any of them.  Defaults: 128, 128,
+ * 128, 1024, 16, 1, 0, 0, 0.  Set them while no call of that family runs
+ * (they are read at each launch). */
 typedef struct {
     uint32_t verify_chain_block;
     uint32_t keygen_chain_block;
@@ -144,6 +208,8 @@ typedef struct {
     uint32_t short_hmsg_blocks;
     uint32_t prep_split;
     uint32_t persist_sort;
+    uint32_t persist_extra_ctas;
+    uint32_t persist_hmsg_sms;
 } xmss_b200_tuning;
 
 int xmss_b200_tuning_get(unsigned int func, unsigned int n, xmss_b200_tuning *out);
