@@ -466,6 +466,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         sec["keygen"] = keygen_rate(xb, torch, dev, sh)
     if world == 1 and not args.skip_mix:
         sec["mix"] = mix_rates(xb, torch, dev, sh)
+    if world == 1 and not args.skip_batch:
+        sec["batch"] = batch_rates(xb, torch, dev, sh)
     if world == 1 and not args.skip_serve:
         sargs = argparse.Namespace(**vars(args))
         sargs.serve_rates, sargs.serve_n, sargs.serve_seconds = args.sec_serve_rates, 30000, 1.0
@@ -896,6 +898,141 @@ def mix_rates(xb, torch, dev, sh):
     return out
 
 
+# Mixed batch (one CUDA graph over several parameter sets and all three kinds):
+# (kind, set name, XMSS^MT, items, keys).  Sign groups sign runs of
+# consecutive indices per key (a key's subtree is built once per batch).
+BATCH_GROUPS = (("keygen", "XMSS-SHA2_10_256", False, 16, 16),
+                ("keygen", "XMSSMT-SHA2_20/4_256", True, 64, 64),
+                ("sign", "XMSS-SHA2_10_256", False, 1024, 16),
+                ("sign", "XMSSMT-SHA2_20/4_256", True, 512, 8),
+                ("verify", "XMSS-SHA2_10_256", False, 2048, 32),
+                ("verify", "XMSS-SHAKE_10_256", False, 512, 8),
+                ("verify", "XMSSMT-SHA2_20/4_256", True, 512, 8))
+
+
+def _batch_inputs(xb, torch, dev, rng):
+    """Device buffers and batch-group dicts of BATCH_GROUPS, with what each
+    group must produce (made by the per-kind entry points of this library)."""
+    groups, expect, keep = [], [], []
+    for kind, name, mt, count, nkeys in BATCH_GROUPS:
+        oid = xb.xmssmt_str_to_oid(name) if mt else xb.xmss_str_to_oid(name)
+        p = xb.parse_oid(oid, mt)
+        n = p.n
+        seeds = np.frombuffer(rng.bytes(nkeys * 3 * n), np.uint8).reshape(nkeys, 3 * n)
+        if kind == "keygen":
+            pks, sks = xb.keypair_batch(oid, mt, seeds)
+            d_seeds = torch.from_numpy(seeds.copy()).to(dev)
+            d_pk = torch.zeros((count, 2 * n), dtype=torch.uint8, device=dev)
+            d_sk = torch.zeros((count, p.sk_bytes), dtype=torch.uint8, device=dev)
+            keep += [d_seeds, d_pk, d_sk]
+            groups.append(dict(kind=xb.KEYGEN, oid=oid, mt=int(mt), count=count, d_seeds=d_seeds.data_ptr(),
+                               d_pk=d_pk.data_ptr(), d_sk=d_sk.data_ptr()))
+            expect.append(("keygen", np.ascontiguousarray(pks[:, 4:]), np.ascontiguousarray(sks[:, 4:]), d_pk, d_sk))
+            continue
+        pks, sks = xb.keypair_batch(oid, mt, seeds)
+        per = count // nkeys
+        msgs = [rng.bytes(int(L)) for L in np.exp(rng.uniform(np.log(32), np.log(1024), count)).astype(int)]
+        rows = np.array(sks[np.arange(count) // per])
+        for k in range(nkeys):
+            start = int(rng.integers(0, (1 << p.full_height) - per - 1))
+            for i in range(per):
+                rows[k * per + i, 4:4 + p.index_bytes] = np.frombuffer((start + i).to_bytes(p.index_bytes, "big"),
+                                                                      np.uint8)
+        if kind == "sign":
+            ret, want = xb.sign_batch(mt, rows.copy(), msgs)
+            smbuf, smoff, _ = xb.pack([bytes(p.sig_bytes) + m for m in msgs], align=16)
+            d_sm = torch.from_numpy(smbuf).to(dev)
+            d_off = torch.from_numpy(smoff.astype(np.int64)).to(dev)
+            d_len = torch.from_numpy(np.array([len(m) for m in msgs], np.int64)).to(dev)
+            keep += [d_sm, d_off, d_len]
+            groups.append(dict(kind=xb.SIGN, oid=oid, mt=int(mt), count=count, sk=rows, d_sm=d_sm.data_ptr(),
+                               d_sm_off=d_off.data_ptr(), d_len=d_len.data_ptr()))
+            expect.append(("sign", want, smoff, d_sm))
+            continue
+        ret, sms = xb.sign_batch(mt, rows.copy(), msgs)
+        sms = [bytearray(x) for x in sms]
+        bad = rng.choice(count, count // 10, replace=False)
+        for i in bad:
+            sms[i][int(rng.integers(0, len(sms[i])))] ^= 1 << int(rng.integers(0, 8))
+        want = np.zeros(count, np.int32)
+        want[bad] = -1
+        buf, off, ln = xb.pack([bytes(x) for x in sms], align=16)
+        d_sm = torch.from_numpy(buf).to(dev)
+        d_off = torch.from_numpy(off.astype(np.int64)).to(dev)
+        d_len = torch.from_numpy(ln.astype(np.int64)).to(dev)
+        d_pk = torch.from_numpy(np.ascontiguousarray(pks[:, 4:])).to(dev)
+        d_kix = torch.from_numpy((np.arange(count) // per).astype(np.int32)).to(dev)
+        d_st = torch.full((count,), 99, dtype=torch.int32, device=dev)
+        keep += [d_sm, d_off, d_len, d_pk, d_kix, d_st]
+        groups.append(dict(kind=xb.VERIFY, oid=oid, mt=int(mt), count=count, d_sm=d_sm.data_ptr(),
+                           d_sm_off=d_off.data_ptr(), d_len=d_len.data_ptr(), d_pk=d_pk.data_ptr(), npk=nkeys,
+                           d_pk_index=d_kix.data_ptr(), d_status=d_st.data_ptr()))
+        expect.append(("verify", want, d_st))
+    return groups, expect, keep
+
+
+def _fresh(groups):
+    """The groups with copies of the sign groups' host keys (create advances them)."""
+    return [dict(g, sk=g["sk"].copy()) if "sk" in g else dict(g) for g in groups]
+
+
+def batch_rates(xb, torch, dev, sh, repeats: int = 5):
+    """One CUDA graph of keygen, sign and verify groups of three parameter
+    sets (two hash families, XMSS and XMSS^MT), timed per launch with CUDA
+    events (L2 flushed before each), against the same groups captured one
+    per graph and launched back to back on one stream; outputs checked
+    byte for byte against the per-kind entry points."""
+    rng = np.random.default_rng(SEED + 5)
+    groups, expect, keep = _batch_inputs(xb, torch, dev, rng)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.ExternalStream(sh)
+
+    def timed(batches):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for b in batches:
+            assert b.launch(sh) == 0
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    one, seq = [], []
+    for _ in range(repeats):
+        b = xb.Batch(_fresh(groups))
+        one.append(timed([b]))
+        b.close()
+        bs = [xb.Batch(_fresh([g])) for g in groups]
+        seq.append(timed(bs))
+        for x in bs:
+            x.close()
+    # outputs of the last sequential launch overwritten by one more batched launch, then checked
+    b = xb.Batch(_fresh(groups))
+    assert b.launch(sh) == 0
+    torch.cuda.synchronize()
+    b.close()
+    ok = True
+    for e in expect:
+        if e[0] == "keygen":
+            ok &= e[3].cpu().numpy().tobytes() == e[1].tobytes() and e[4].cpu().numpy().tobytes() == e[2].tobytes()
+        elif e[0] == "sign":
+            sm = e[3].cpu().numpy()
+            ok &= all(sm[int(o):int(o) + len(w)].tobytes() == w for w, o in zip(e[1], e[2]))
+        else:
+            ok &= bool((e[2].cpu().numpy() == e[1]).all())
+    items = sum(g[3] for g in BATCH_GROUPS)
+    ms, ms_seq = float(np.median(one)), float(np.median(seq))
+    out = {"workload": "mixed batch, one CUDA graph",
+           "groups": [{"kind": k, "set": nm, "items": c} for k, nm, _, c, _ in BATCH_GROUPS],
+           "items": items, "ms_per_batch": ms, "items_per_s": items / (ms / 1e3),
+           "ms_groups_one_graph_each_back_to_back": ms_seq, "repeats": repeats,
+           "correct": bool(ok), "check": "every key, signature and status equal to the per-kind entry points "
+                                        "(keypair_batch, sign_batch, expected accept bitmap)"}
+    log(out)
+    return out
+
+
 def run_plain(args):
     """Config 1 and the per-call baseline: XMSS-SHA2_10_256 keypair from a
     seeded seed, then 16 x (xmss_sign, xmss_sign_open) of 32-byte messages,
@@ -1186,6 +1323,7 @@ def main():
                     help="offered rates of the short serving sweep in the default line")
     ap.add_argument("--skip-keygen", action="store_true")
     ap.add_argument("--skip-mix", action="store_true")
+    ap.add_argument("--skip-batch", action="store_true")
     ap.add_argument("--skip-serve", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=2.5)

@@ -707,12 +707,6 @@ extern "C" int xmss_b200_rate_probe(int kind, uint32_t blocks, uint32_t iters, u
     });
 }
 
-extern "C" int xmss_b200_persist_trace(double* out, uint32_t max_kinds)
-{
-    if (!out) return kBad;
-    return guarded([&](Engine& e) { return e.persist_trace(out, max_kinds); });
-}
-
 extern "C" int xmss_b200_last_verify_work(xmss_b200_work* out)
 {
     return guarded([&](Engine& e) {

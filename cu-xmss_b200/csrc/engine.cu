@@ -498,82 +498,28 @@ void Engine::verify_persistent(const FamilyOps* ops, const xmss_params& p, uint3
     v.sig_bytes = p.sig_bytes;
     v.tree_height = p.tree_height;
     v.d = d;
-    // state: ticket (8 B), header, then per (group, layer) ntot /
-    // chains_done / gate / 8 L-tree level counters, per group h_pre
-    // counters, the H_msg length histogram and bucket cursors, and the
-    // ready queue (8-byte entries); all of it starts at zero
+    // state: ticket (8 B), header, then per (group, layer) ready / ntot /
+    // chains_done / 8 L-tree level counters, then per group h_pre counters
     const size_t gl = (size_t)groups * d;
-    const size_t words = kPersistHdrWords + gl * 11 + groups + 2 * kSortBuckets + kPersistSmSlots;
-    const unsigned long long cap = persist_rq_cap(count, d, (int)len);
-    const size_t rq_off = (8 + words * 4 + 7) & ~(size_t)7;
-    const unsigned long long cap_hi = persist_rqh_cap(count, d, (int)len);
-    // queue slots are 32-bit, the top two values mark "none"; groups are 24-bit in a task word
-    if (cap >= 0xFFFFFFF0ull || cap_hi >= 0xFFFFFFF0ull || groups >= (1u << 24))
-        throw CudaFailure("batch too large for one persistent launch");
-    const size_t state_bytes = rq_off + (cap + cap_hi) * 8;
-    uint8_t* st8 = w.pstate.as<uint8_t>(state_bytes);
+    const size_t words = 4 + gl * 11 + groups;
+    uint8_t* st8 = w.pstate.as<uint8_t>(8 + words * 4);
     uint32_t* u = (uint32_t*)(st8 + 8);
     PersistArgs q{};
     q.ticket = (unsigned long long*)st8;
     q.hdr = u;
-    q.ntot = u + kPersistHdrWords;
+    q.ready = u + 4;
+    q.ntot = q.ready + gl;
     q.chains_done = q.ntot + gl;
-    q.gate = q.chains_done + gl;
-    q.lt_done = q.gate + gl;
+    q.lt_done = q.chains_done + gl;
     q.hpre_done = q.lt_done + 8 * gl;
-    q.sort = q.hpre_done + groups;
-    q.smctr = q.sort + 2 * kSortBuckets;
-    q.rq = (unsigned long long*)(st8 + rq_off);
-    q.rq_cap = cap;
-    q.rqh = q.rq + cap;
-    q.rqh_cap = cap_hi;
-    q.perm = w.aux.as<uint32_t>(count);
     q.list = w.list.as<uint32_t>((size_t)groups * 32 * len);
     q.ctx = w.ctx.get((size_t)npk * ops->ctx_bytes);
     q.npk = npk;
     q.groups = groups;
     q.wait_ns = persist_wait_ns;
-    q.short_blocks = tuning_for(ops->func, ops->n).short_hmsg_blocks;
-    q.sorted = tuning_for(ops->func, ops->n).persist_sort;
-    // one H_msg CTA on each of the first SMs: four groups at a time per SM,
-    // at most a quarter of the SMs
-    q.hmsg_sms = 0;
-    if (tuning_for(ops->func, ops->n).persist_hmsg_sms) {
-        int sms = 0;
-        XB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
-        q.hmsg_sms = std::min<uint32_t>((groups + 3) / 4, (uint32_t)std::max(1, sms / 4));
-    }
-    XB_CUDA(cudaMemsetAsync(st8, 0, state_bytes, st));
-    q.trace = nullptr;
-    ptrace_last_ = nullptr;
-    if (profiling) {
-        q.trace = ptrace_.as<unsigned long long>(4 * kTrKinds);
-        XB_CUDA(cudaMemsetAsync(q.trace, 0, 4 * kTrKinds * sizeof(unsigned long long), st));
-        ptrace_last_ = q.trace;
-    }
+    XB_CUDA(cudaMemsetAsync(st8, 0, 8 + words * 4, st));
     ops->verify_persist(v, q, st);
     XB_CUDA(cudaGetLastError());
-}
-
-int Engine::persist_trace(double* out, uint32_t max_kinds)
-{
-    if (!ptrace_last_) return -1;
-    XB_CUDA(cudaSetDevice(device_));
-    if (have_done_) XB_CUDA(cudaEventSynchronize(done_));
-    unsigned long long r[4 * kTrKinds];
-    XB_CUDA(cudaMemcpy(r, ptrace_last_, sizeof r, cudaMemcpyDeviceToHost));
-    unsigned long long t0 = ~0ull;
-    for (uint32_t k = 0; k < kTrKinds; k++)
-        if (r[4 * k + 3]) t0 = std::min(t0, ~r[4 * k]);
-    const uint32_t n = std::min<uint32_t>(max_kinds, kTrKinds);
-    for (uint32_t k = 0; k < n; k++) {
-        const bool any = r[4 * k + 3] != 0;
-        out[4 * k] = any ? (double)(~r[4 * k] - t0) / 1e3 : 0;
-        out[4 * k + 1] = any ? (double)(r[4 * k + 1] - t0) / 1e3 : 0;
-        out[4 * k + 2] = (double)r[4 * k + 2] / 1e3;
-        out[4 * k + 3] = (double)r[4 * k + 3];
-    }
-    return (int)n;
 }
 
 void Engine::last_verify_work(unsigned long long out[3])

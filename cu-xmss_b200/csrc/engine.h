@@ -223,11 +223,6 @@ class Engine {
     // Work counters of the last verify (see xmss_b200_last_verify_work).
     void last_verify_work(unsigned long long out[3]);
 
-    // Task trace of the last persistent verify made while profiling
-    // (xmss_b200_persist_trace): kinds x [first start us, last end us,
-    // busy warp-us, tasks]; returns the kinds written, -1 without a trace.
-    int persist_trace(double* out, uint32_t max_kinds);
-
     // Phase timing (xmss_b200_profile / xmss_b200_phase_ms).
     enum Phase { kPrep = 0, kChains = 1, kLtree = 2, kRoot = 3, kTree = 4, kPhases = 5 };
     bool profiling = false;
@@ -247,8 +242,6 @@ class Engine {
     Workspace ws_;  // scratch of the engine's own entry points
     DevBuf s_work_;
     unsigned long long* work_ = nullptr;
-    DevBuf ptrace_;                         // trace of the last persistent verify (profiling)
-    unsigned long long* ptrace_last_ = nullptr;
     struct Mark {
         int phase;
         cudaEvent_t a, b;

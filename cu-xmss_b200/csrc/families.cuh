@@ -1201,59 +1201,6 @@ __device__ __forceinline__ void hmsg_sha256_n32(uint32_t (&out)[8], const uint32
     for (int i = 0; i < 8; i++) out[i] = st[i];
 }
 
-// The same H_msg in the register-lean form of the persistent kernels: one
-// compression body in a rolled loop over every block (the two prefix
-// blocks, the whole message blocks, the padded tail), each block assembled
-// when it is consumed (no block loaded ahead) and R and the root read from
-// memory for their block.  Its peak register use stays near a chain's, so
-// a kernel that also runs chains keeps the chains' occupancy; per block it
-// is slower than hmsg_sha256_n32.  R: n bytes (the signature's R), root: n
-// bytes (the public root); big-endian words as F::load gives them.
-__device__ __forceinline__ void hmsg_sha256_n32_lean(uint32_t (&out)[8], const uint8_t* Rp, const uint8_t* rootp,
-                                                     uint64_t idx, const uint8_t* m, uint64_t mlen)
-{
-    const uint64_t nfull = mlen / 64;
-    const uint64_t o0 = 64 * nfull;
-    const uint64_t nb = 2 + nfull + (((mlen - o0) + 9 > 64) ? 2 : 1);
-    const uint64_t L = 128 + mlen;
-    uint32_t st[8];
-    sha256_iv(st);
-#pragma unroll 1
-    for (uint64_t b = 0; b < nb; b++) {
-        uint32_t w[16];
-        if (b < 2) {  // toByte(2, 32) || R, then root || toByte(idx, 32)
-            uint32_t v[8];
-            Sha256N32T<0>::load(v, b == 0 ? Rp : rootp);
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                w[i] = b == 0 ? (i == 7 ? 2u : 0u) : v[i];
-                w[8 + i] = b == 0 ? v[i] : 0u;
-            }
-            if (b == 1) {
-                w[14] = (uint32_t)(idx >> 32);
-                w[15] = (uint32_t)idx;
-            }
-        } else if (b < 2 + nfull) {
-            load_block64_be(w, m, mlen, 64 * (b - 2));
-        } else {  // the end of M, the 0x80 byte and the length
-#pragma unroll
-            for (int j = 0; j < 16; j++) {
-                const uint64_t o = 64 * (b - 2) + 4 * j;
-                uint32_t le = (o < mlen) ? fetch4_le(m, mlen, o) : 0;
-                if (o <= mlen && mlen < o + 4) le |= 0x80u << (8 * (mlen - o));
-                w[j] = bswap32(le);
-            }
-            if (b == nb - 1) {
-                w[14] = (uint32_t)((L * 8) >> 32);
-                w[15] = (uint32_t)(L * 8);
-            }
-        }
-        sha256_compress(st, w);
-    }
-#pragma unroll
-    for (int i = 0; i < 8; i++) out[i] = st[i];
-}
-
 template <class F>
 __device__ void hmsg(uint32_t (&out)[F::NW], const uint32_t (&R)[F::NW], const uint32_t (&root)[F::NW],
                      uint64_t idx, const uint8_t* m, uint64_t mlen)

@@ -165,28 +165,19 @@ struct Launch {
         if (!v.count) return;
         launch_pdl(k_verify_root<F>, (v.count + 63) / 64, 64, st, v, layer);
     }
-    // as many CTAs as fit on the GPU at once: each loops over the queues
-    // (more would only wait behind them; fewer leave SMs idle)
-    template <int EXTRA>
-    static void persist_launch(const VerifyArgs& v, const PersistArgs& q, cudaStream_t st)
+    static void verify_persist(const VerifyArgs& v, const PersistArgs& q, cudaStream_t st)
     {
+        if (!v.count) return;
+        // as many CTAs as fit on the GPU at once: each loops over the ticket
+        // sequence (more would only queue behind them; fewer leave SMs idle)
         static const unsigned grid = [] {
             int dev = 0, sms = 0, per = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_verify_persist<F, FT, EXTRA>, 128, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_verify_persist<F, FT>, 128, 0);
             return (unsigned)(sms * (per > 0 ? per : 1));
         }();
-        k_verify_persist<F, FT, EXTRA><<<grid, 128, 0, st>>>(v, q);
-    }
-    static void verify_persist(const VerifyArgs& v, const PersistArgs& q, cudaStream_t st)
-    {
-        if (!v.count) return;
-        switch (tune().persist_extra_ctas) {
-            case 1: persist_launch<1>(v, q, st); break;
-            case 2: persist_launch<2>(v, q, st); break;
-            default: persist_launch<0>(v, q, st); break;
-        }
+        k_verify_persist<F, FT><<<grid, 128, 0, st>>>(v, q);
     }
     static void sign_prep(const SignArgs& g, const void* ctx, cudaStream_t st)
     {

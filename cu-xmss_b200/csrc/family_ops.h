@@ -63,9 +63,6 @@ struct Tuning {
     uint32_t split_min = 1024;          // verify batches this large run as two groups ...
     uint32_t short_hmsg_blocks = 16;    // ... split at this many H_msg blocks
     uint32_t prep_split = 1;            // split batches: h_pre in its own launch (1) or in each group's prep (0)
-    uint32_t persist_sort = 1;          // persistent verify: groups sorted by H_msg length (1) or batch order (0)
-    uint32_t persist_extra_ctas = 0;    // persistent verify: resident CTAs per SM above the spill-free count (0..2)
-    uint32_t persist_hmsg_sms = 1;      // persistent verify: H_msg first on reserved SMs (1) or mixed in (0)
 };
 Tuning& tuning_for(unsigned func, unsigned n);
 

@@ -73,9 +73,6 @@ void to_c(const xb::Tuning& t, xmss_b200_tuning* o)
     o->split_min = t.split_min;
     o->short_hmsg_blocks = t.short_hmsg_blocks;
     o->prep_split = t.prep_split;
-    o->persist_sort = t.persist_sort;
-    o->persist_extra_ctas = t.persist_extra_ctas;
-    o->persist_hmsg_sms = t.persist_hmsg_sms;
 }
 
 }  // namespace
@@ -90,8 +87,7 @@ extern "C" int xmss_b200_tuning_get(unsigned func, unsigned n, xmss_b200_tuning*
 extern "C" int xmss_b200_tuning_set(unsigned func, unsigned n, const xmss_b200_tuning* t)
 {
     if (!xb::family_ops(func, n) || !t || !block_ok(t->verify_chain_block) || !block_ok(t->keygen_chain_block) ||
-        !block_ok(t->level_block) || !t->split_min || !t->short_hmsg_blocks || t->prep_split > 1 ||
-        t->persist_sort > 1 || t->persist_extra_ctas > 2 || t->persist_hmsg_sms > 1) {
+        !block_ok(t->level_block) || !t->split_min || !t->short_hmsg_blocks || t->prep_split > 1) {
         xb::set_last_error("xmss_b200_tuning_set: unknown family or shape out of range");
         return -1;
     }
@@ -103,9 +99,6 @@ extern "C" int xmss_b200_tuning_set(unsigned func, unsigned n, const xmss_b200_t
     d.split_min = t->split_min;
     d.short_hmsg_blocks = t->short_hmsg_blocks;
     d.prep_split = t->prep_split;
-    d.persist_sort = t->persist_sort;
-    d.persist_extra_ctas = t->persist_extra_ctas;
-    d.persist_hmsg_sms = t->persist_hmsg_sms;
     return 0;
 }
 

@@ -117,12 +117,13 @@ lib.xmss_b200_verify_graph_create.argtypes = [C.c_uint32, C.c_int, C.c_uint32] +
 lib.xmss_b200_verify_graph_launch.argtypes = [C.c_void_p, C.c_void_p]
 lib.xmss_b200_verify_graph_destroy.argtypes = [C.c_void_p]
 lib.xmss_b200_verify_graph_destroy.restype = None
+
+
 class Tuning(C.Structure):
     """xmss_b200_tuning (include/xmss_b200.h)."""
 
     _fields_ = [(k, C.c_uint32) for k in ("verify_chain_block", "keygen_chain_block", "level_block", "split_min",
-                                          "short_hmsg_blocks", "prep_split", "persist_sort",
-                                          "persist_extra_ctas", "persist_hmsg_sms")]
+                                          "short_hmsg_blocks", "prep_split")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -138,21 +139,6 @@ lib.xmss_b200_last_verify_work.argtypes = [C.POINTER(Work)]
 lib.xmss_b200_sign_open_device_noalloc.argtypes = lib.xmss_b200_sign_open_device.argtypes
 lib.xmss_b200_sign_open_device_persistent.argtypes = lib.xmss_b200_sign_open_device.argtypes
 lib.xmss_b200_set_wait_bound.argtypes = [C.c_ulonglong]
-lib.xmss_b200_persist_trace.argtypes = [C.POINTER(C.c_double), C.c_uint32]
-
-PERSIST_TRACE_KINDS = ("count", "ctx", "prefix", "scatter", "hmsg", "hpre", "chain", "ltree", "root", "idle")
-
-
-def persist_trace() -> dict | None:
-    """xmss_b200_persist_trace: per task kind of the last persistent verify
-    made while profiling, {first_us, last_us, busy_warp_us, tasks}."""
-    buf = (C.c_double * (4 * len(PERSIST_TRACE_KINDS)))()
-    n = _check(lib.xmss_b200_persist_trace(buf, len(PERSIST_TRACE_KINDS)), "persist_trace")
-    if n < 0:
-        return None
-    return {PERSIST_TRACE_KINDS[k]: {"first_us": buf[4 * k], "last_us": buf[4 * k + 1],
-                                     "busy_warp_us": buf[4 * k + 2], "tasks": int(buf[4 * k + 3])}
-            for k in range(n)}
 lib.xmss_b200_profile.argtypes = [C.c_int]
 lib.xmss_b200_phase_ms.argtypes = [C.POINTER(C.c_double)]
 lib.xmss_b200_rate_probe.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]

@@ -187,19 +187,9 @@ void xmss_b200_batch_destroy(xmss_b200_batch *b);
  * batch, prep_split = 1 runs the L-tree precomputation (h_pre) of both
  * groups as a launch of its own on a third stream, so that each group's
  * chains wait only for its H_msg; 0 runs it inside each group's prep
- * launch.  persist_sort = 1 makes the persistent verify group its
- * signatures by H_msg length (a device counting sort at the head of its
- * queue; longest H_msg first, the other tasks shortest first, chains in
- * two bands split at short_hmsg_blocks); 0 keeps them in batch order.
- * persist_extra_ctas (0, 1, 2) raises the persistent verify's resident
- * CTAs per SM above its spill-free count, trading register spills for
- * occupancy.  persist_hmsg_sms = 1 starts the persistent verify with one
- * CTA of H_msg tasks on each of the first SMs (four groups at a time per
- * SM, one per sub-partition, at most a quarter of the SMs) while the other
- * CTAs there wait for H_msg to finish, so the serial H_msg chains run
- * nearly alone.  Results do not depend on any of them.  Defaults: 128, 128,
- * 128, 1024, 16, 1, 0, 0, 0.  Set them while no call of that family runs
- * (they are read at each launch). */
+ * launch.  Results do not depend on any of them.  Defaults: 128, 128,
+ * 128, 1024, 16, 1.  Set them while no call of that family runs (they are
+ * read at each launch). */
 typedef struct {
     uint32_t verify_chain_block;
     uint32_t keygen_chain_block;
@@ -207,9 +197,6 @@ typedef struct {
     uint32_t split_min;
     uint32_t short_hmsg_blocks;
     uint32_t prep_split;
-    uint32_t persist_sort;
-    uint32_t persist_extra_ctas;
-    uint32_t persist_hmsg_sms;
 } xmss_b200_tuning;
 
 int xmss_b200_tuning_get(unsigned int func, unsigned int n, xmss_b200_tuning *out);
@@ -300,16 +287,6 @@ int xmss_b200_last_verify_work(xmss_b200_work *out);
  * [4] Merkle tree levels (keygen, sign).  Off by default. */
 int xmss_b200_profile(int enable);
 int xmss_b200_phase_ms(double ms[5]);
-
-/* Task trace of the last xmss_b200_sign_open_device_persistent call made
- * while profiling was enabled: for each task kind of the launch (count,
- * ctx, prefix, scatter, hmsg, hpre, chain, ltree, root, and idle = a warp
- * waiting for its next ready task) four values in out[4 * kind ..]: the
- * first start and the last end in us after the launch's first task, the
- * summed busy warp-us, and the tasks.  Waits for that call.  Returns the
- * kinds written (at most max_kinds), -1 when there is no trace.  No
- * reference counterpart (observability of the persistent launch). */
-int xmss_b200_persist_trace(double *out, uint32_t max_kinds);
 
 /* Same as xmss_b200_sign_open_device, but allocates nothing: no
  * reference counterpart; it exists for callers that cannot allocate device
