@@ -1236,14 +1236,19 @@ def run_serve(args):
             "pk": pkt, "pk_stride": pk_stride}
     log("serve: pool ready", srv.stats())
 
+    rates = [float(r) for r in args.serve_rates.split(",")]
     # warm-up (untimed): a burst that grows every slot's and lane's buffers
-    # to their working size before the sweep
+    # to their working size, then a short trace at the lowest rate, whose
+    # small batches take the launch forms of small batches (the CUDA runtime
+    # loads each kernel at its first launch: tens of ms inside the sweep)
     tr, keep = _serve_trace(xb, rng, args.serve_n // 2, 0.0, keys, kids, pool, rand)
+    ret, _, _, _ = srv.replay(tr)
+    assert (ret == 0).all()
+    tr, keep = _serve_trace(xb, rng, 2000, min(rates), keys, kids, pool, rand)
     ret, _, _, _ = srv.replay(tr)
     assert (ret == 0).all()
     log("serve: warm", srv.stats())
 
-    rates = [float(r) for r in args.serve_rates.split(",")]
     sweep = []
     oracle_check = None
     for rate in rates + [0.0]:

@@ -1102,6 +1102,55 @@ __device__ void hmsg_shake(uint32_t (&out)[F::NW], const HMsgPrefix<F>& pre, con
     for (int i = 0; i < F::NW; i++) out[i] = (i & 1) ? (uint32_t)(A[i / 2] >> 32) : (uint32_t)A[i / 2];
 }
 
+// H_msg of ONE message by a whole warp (SHAKE families), every lane taking
+// part: lane t < RATEW / 2 absorbs the 64-bit word t of each rate block (its
+// loads of the next block are issued before the current permutation), and
+// keccak_f1600_warp runs the permutation across the lanes.  Same bytes as
+// hmsg_shake (prefix || M, pad 0x1F ... 0x80); every lane gets the digest.
+template <class F, int RATEW>
+__device__ void hmsg_shake_warp(uint32_t (&out)[F::NW], const HMsgPrefix<F>& pre, const uint8_t* m, uint64_t mlen)
+{
+    constexpr int W = HMsgPrefix<F>::W;
+    const uint64_t L = 4ull * W + mlen;
+    const uint64_t nb = L / (4 * RATEW) + 1;
+    const uint32_t lane = threadIdx.x & 31;
+    const KeccakWarpLane kl;
+    // word s (4 bytes at offset 4s) of the padded stream, little-endian
+    auto word = [&](uint64_t s) -> uint32_t {
+        const uint64_t o = 4 * s;
+        uint32_t v = 0;
+        if (s < (uint64_t)W) {
+#pragma unroll
+            for (int i = 0; i < W; i++)
+                if ((uint64_t)i == s) v = pre.w[i];
+        } else if (o < L) {
+            v = fetch4_le(m, mlen, o - 4ull * W);
+        }
+        if (o <= L && L < o + 4) v |= 0x1Fu << (8 * (L - o));
+        return v;
+    };
+    uint32_t lo = 0, hi = 0, nl = 0, nh = 0;
+    if (lane < RATEW / 2) {
+        nl = word(2 * lane);
+        nh = word(2 * lane + 1);
+    }
+    for (uint64_t b = 0; b < nb; b++) {
+        if (lane < RATEW / 2) {
+            lo ^= nl;
+            hi ^= nh;
+            if (b + 1 == nb && lane == RATEW / 2 - 1) hi ^= 0x80000000u;
+            if (b + 1 < nb) {
+                const uint64_t s = (b + 1) * RATEW + 2 * lane;
+                nl = word(s);
+                nh = word(s + 1);
+            }
+        }
+        keccak_f1600_warp(lo, hi, kl);
+    }
+#pragma unroll
+    for (int i = 0; i < F::NW; i++) out[i] = __shfl_sync(0xffffffffu, (i & 1) ? hi : lo, i / 2);
+}
+
 template <class F> struct HMsgKind;
 template <int M> struct HMsgKind<Sha256N32T<M>> { static constexpr int v = 0; };
 template <> struct HMsgKind<Sha256N24> { static constexpr int v = 0; };
@@ -1217,6 +1266,21 @@ __device__ void hmsg(uint32_t (&out)[F::NW], const uint32_t (&R)[F::NW], const u
             hmsg_shake<F, K>(out, pre, m, mlen);
         }
     }
+}
+
+// H_msg by a whole warp (one message per warp) for the families whose
+// permutation has a warp form (SHAKE); kWarpHmsg<F> says which.
+template <class F>
+constexpr bool kWarpHmsg = HMsgKind<F>::v >= 34;
+
+template <class F>
+__device__ void hmsg_warp(uint32_t (&out)[F::NW], const uint32_t (&R)[F::NW], const uint32_t (&root)[F::NW],
+                          uint64_t idx, const uint8_t* m, uint64_t mlen)
+{
+    static_assert(kWarpHmsg<F>, "warp H_msg is the SHAKE form");
+    HMsgPrefix<F> pre;
+    pre.build(R, root, idx);
+    hmsg_shake_warp<F, HMsgKind<F>::v>(out, pre, m, mlen);
 }
 
 }  // namespace xb

@@ -109,14 +109,25 @@ struct Launch {
     static void verify_prep(const VerifyArgs& v, const void* ctx, cudaStream_t st)
     {
         if (!v.count) return;
-        const uint32_t hb = (v.count + 63) / 64;
         const uint64_t pre = (uint64_t)v.count * v.d * (F::LEN - 1 + v.tree_height);
+        if constexpr (kWarpHmsg<F>) {
+            // H_msg one warp per signature, beside the h_pre blocks
+            const uint32_t hw = (v.count + 1) / 2;
+            k_verify_hmsg_warp<F><<<(unsigned)(hw + (pre + 63) / 64), 64, 0, st>>>(v, hw, (const Ctx*)ctx);
+            return;
+        }
+        const uint32_t hb = (v.count + 63) / 64;
         k_verify_prep<F><<<(unsigned)(hb + (pre + 63) / 64), 64, 0, st>>>(v, hb, (const Ctx*)ctx);
     }
     static void verify_prep_part(const VerifyArgs& v, const void* ctx, cudaStream_t st, int part)
     {
         if (!v.count) return;
         if (part == 1) {
+            if constexpr (kWarpHmsg<F>) {
+                const uint32_t hw = (v.count + 1) / 2;
+                k_verify_hmsg_warp<F><<<hw, 64, 0, st>>>(v, hw, (const Ctx*)ctx);
+                return;
+            }
             const uint32_t hb = (v.count + 63) / 64;
             k_verify_prep<F><<<hb, 64, 0, st>>>(v, hb, (const Ctx*)ctx);
             return;
@@ -182,6 +193,11 @@ struct Launch {
     static void sign_prep(const SignArgs& g, const void* ctx, cudaStream_t st)
     {
         if (!g.count) return;
+        if constexpr (kWarpHmsg<F>) {
+            k_sign_hmsg_warp<F><<<(g.count + 1) / 2, 64, 0, st>>>(g, (const Ctx*)ctx);
+            k_sign_prep<F, true><<<(g.count + 63) / 64, 64, 0, st>>>(g, (const Ctx*)ctx);
+            return;
+        }
         k_sign_prep<F><<<(g.count + 63) / 64, 64, 0, st>>>(g, (const Ctx*)ctx);
     }
     static void sign_chains(const SignArgs& g, const void* ctx, cudaStream_t st)

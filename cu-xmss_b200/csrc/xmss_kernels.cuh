@@ -516,6 +516,56 @@ __global__ void __launch_bounds__(64) k_verify_prep(VerifyArgs v, uint32_t hmsg_
     verify_hpre_item<F>(v, ctx, (uint64_t)(blockIdx.x - hmsg_blocks_n) * blockDim.x + threadIdx.x);
 }
 
+// The H_msg part of k_verify_prep with one WARP per signature, for the
+// families with a warp-parallel permutation (kWarpHmsg: SHAKE).  H_msg is a
+// serial chain of permutations, so a batch's prep lasts as long as its
+// longest message; spread over a warp the chain runs about four times
+// faster.  Two signatures per 64-thread block; same outputs as the thread
+// form (digest, chain lengths, index, status, step histogram, work).  As in
+// k_verify_prep, blocks from hmsg_blocks_n on compute h_pre items instead.
+template <class F>
+__global__ void __launch_bounds__(64) k_verify_hmsg_warp(VerifyArgs v, uint32_t hmsg_blocks_n,
+                                                         const typename F::Ctx* __restrict__ ctx)
+{
+    if (blockIdx.x >= hmsg_blocks_n) {
+        verify_hpre_item<F>(v, ctx, (uint64_t)(blockIdx.x - hmsg_blocks_n) * blockDim.x + threadIdx.x);
+        return;
+    }
+    __shared__ uint32_t sh_hist[16];
+    if (threadIdx.x < 16) sh_hist[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t i = blockIdx.x * 2 + (threadIdx.x >> 5);
+    const uint32_t lane = threadIdx.x & 31;
+    if (i < sel_count(v)) {
+        const uint32_t s = sel_sig(v, i);
+        const uint64_t smlen = v.smlen[s];
+        if (!verify_input_ok(v, s)) {
+            if (lane == 0) v.status[s] = -1;
+        } else {
+            const uint8_t* sm = v.sm + v.sm_off[s];
+            const uint64_t idx = bytes_be(sm, (int)v.index_bytes);
+            uint32_t R[F::NW], root[F::NW], mh[F::NW];
+            F::load(R, sm + v.index_bytes);
+            F::load(root, v.key_root + (uint64_t)v.key[s] * v.key_stride);
+            hmsg_warp<F>(mh, R, root, idx, sm + v.sig_bytes, smlen - v.sig_bytes);
+            if (lane == 0) {
+                F::store(v.node + (uint64_t)s * F::N, mh);
+                uint8_t* lens = v.lens + (uint64_t)s * F::LEN;
+                chain_lengths<F>(lens, mh);
+                v.idx[s] = idx;
+                v.status[s] = 0;
+                const unsigned long long steps = count_steps<F>(lens, sh_hist);
+                if (v.work) {
+                    atomicAdd(&v.work[0], hmsg_blocks<F>(smlen - v.sig_bytes));
+                    atomicAdd(&v.work[1], steps);
+                    atomicAdd(&v.work[2], (unsigned long long)(F::LEN - 1 + v.tree_height) * v.d);
+                }
+            }
+        }
+    }
+    flush_hist(sh_hist, v.hist);
+}
+
 // Splits the signatures into a short-H_msg group (at most `blocks_max` hash
 // blocks) and a long one, so the long messages' serial H_msg runs on its own
 // stream while the short group's chains keep the GPU busy.
@@ -811,26 +861,30 @@ struct SignArgs {
 // One thread per signature: R, H_msg, every layer's chain lengths (layer 0
 // signs the message digest, layer i signs the root of layer i-1) and the
 // authentication paths copied out of the subtree node arrays.
-template <class F>
+// HMSG_DONE: R and layer 0's chain lengths were written by k_sign_hmsg_warp.
+template <class F, bool HMSG_DONE = false>
 __global__ void k_sign_prep(SignArgs g, const typename F::Ctx* __restrict__ ctx)
 {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.count) return;
     uint8_t* sm = g.sm + g.sm_off[s];
     const uint64_t idx = g.idx[s];
-    const typename F::Ctx& c = ctx[g.key[s]];
     const uint32_t th = g.tree_height;
-    uint32_t R[F::NW], root[F::NW], mh[F::NW];
-    F::prf_r(R, c, idx);
-    F::store(sm + g.index_bytes, R);
-    F::load(root, g.key_root + (uint64_t)g.key[s] * g.key_stride);
-    hmsg<F>(mh, R, root, idx, g.msg ? g.msg + g.msg_off[s] : sm + g.sig_bytes, g.mlen[s]);
+    uint32_t mh[F::NW];
+    if constexpr (!HMSG_DONE) {
+        const typename F::Ctx& c = ctx[g.key[s]];
+        uint32_t R[F::NW], root[F::NW];
+        F::prf_r(R, c, idx);
+        F::store(sm + g.index_bytes, R);
+        F::load(root, g.key_root + (uint64_t)g.key[s] * g.key_stride);
+        hmsg<F>(mh, R, root, idx, g.msg ? g.msg + g.msg_off[s] : sm + g.sig_bytes, g.mlen[s]);
+    }
     const uint64_t wsb = (uint64_t)F::LEN * F::N;
     for (uint32_t layer = 0; layer < g.d; layer++) {
         const uint8_t* tn = g.nodes + g.tree_off[(uint64_t)s * g.d + layer];
         const uint32_t leaf = (uint32_t)((idx >> (th * layer)) & ((1ull << th) - 1));
         if (layer == 0) {
-            chain_lengths<F>(g.lens + ((uint64_t)s * g.d) * F::LEN, mh);
+            if constexpr (!HMSG_DONE) chain_lengths<F>(g.lens + ((uint64_t)s * g.d) * F::LEN, mh);
         } else {
             uint32_t r[F::NW];
             const uint8_t* prev = g.nodes + g.tree_off[(uint64_t)s * g.d + layer - 1];
@@ -843,6 +897,28 @@ __global__ void k_sign_prep(SignArgs g, const typename F::Ctx* __restrict__ ctx)
             F::load(v, tn + (level_offset((int)th, (int)l) + ((leaf >> l) ^ 1)) * F::N);
             F::store(auth + (uint64_t)l * F::N, v);
         }
+    }
+}
+
+// R and H_msg of each signature with one WARP per signature (kWarpHmsg
+// families: the warp-parallel permutation), writing R into the signature and
+// layer 0's chain lengths; k_sign_prep<F, true> does the rest.  Two
+// signatures per 64-thread block.
+template <class F>
+__global__ void __launch_bounds__(64) k_sign_hmsg_warp(SignArgs g, const typename F::Ctx* __restrict__ ctx)
+{
+    const uint32_t s = blockIdx.x * 2 + (threadIdx.x >> 5);
+    const uint32_t lane = threadIdx.x & 31;
+    if (s >= g.count) return;
+    uint8_t* sm = g.sm + g.sm_off[s];
+    const uint64_t idx = g.idx[s];
+    uint32_t R[F::NW], root[F::NW], mh[F::NW];
+    F::prf_r(R, ctx[g.key[s]], idx);
+    F::load(root, g.key_root + (uint64_t)g.key[s] * g.key_stride);
+    hmsg_warp<F>(mh, R, root, idx, g.msg ? g.msg + g.msg_off[s] : sm + g.sig_bytes, g.mlen[s]);
+    if (lane == 0) {
+        F::store(sm + g.index_bytes, R);
+        chain_lengths<F>(g.lens + ((uint64_t)s * g.d) * F::LEN, mh);
     }
 }
 
