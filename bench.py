@@ -1319,7 +1319,7 @@ def main():
     ap.add_argument("--serve-n", type=int, default=100000, help="most requests per sweep point")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="length of a sweep point")
     ap.add_argument("--serve-batch", type=int, default=4096)
-    ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--serve-plain-n", type=int, default=150, help="requests of the per-call comparison")
     ap.add_argument("--keygen-small", action="store_true", help="keygen workload: one h=16 key (profiling)")
     ap.add_argument("--serve-check", type=int, default=2,

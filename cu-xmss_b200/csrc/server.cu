@@ -208,8 +208,10 @@ struct Plan {
 
 enum class Launch { kLaunched, kNothing, kDeferred };
 
-// Lanes per slot: slots x (lanes + 1) + 1 streams stay within the 32
-// hardware work queues of the device.
+// Lanes per slot.  With 4 slots, slots x (lanes + 1) + 1 streams stay
+// within the 32 hardware work queues of the device; the default 8 slots
+// share queues and still measured the lower p99 (more batches start at
+// once, so requests wait less for a free slot).
 constexpr size_t kMaxLanes = 6;
 
 // Estimated critical path of a plan in microseconds on an idle GPU: the
@@ -1018,7 +1020,7 @@ extern "C" int xmss_b200_server_create(const xmss_b200_server_config* cfg, xmss_
         auto srv = std::make_unique<xmss_b200_server>();
         xmss_b200_server_config c{};
         c.max_batch = 4096;
-        c.slots = 4;
+        c.slots = 8;  // p99 at 100k requests/s: 8.9 ms with 8, 10.2 ms with 4 (B200)
         c.tree_pool_bytes = 1ull << 30;
         c.mem_reserve_bytes = 1ull << 30;
         if (cfg) {

@@ -333,7 +333,7 @@ typedef struct xmss_b200_server xmss_b200_server;
 
 typedef struct {
     uint32_t max_batch;          /* requests per batch (default 4096) */
-    uint32_t slots;              /* batches in flight (default 4) */
+    uint32_t slots;              /* batches in flight (default 8) */
     uint32_t window_us;          /* a free slot waits up to this long for a batch to fill (default 0) */
     uint32_t reserved0;
     uint64_t tree_pool_bytes;    /* device memory of the subtree cache (default 1 GiB) */
