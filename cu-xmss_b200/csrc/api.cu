@@ -620,6 +620,35 @@ extern "C" int xmss_b200_sign_open_device_persistent(uint32_t oid, int mt, uint3
     });
 }
 
+extern "C" int xmss_b200_sign_open_device_persistent_multi(const xmss_b200_verify_job* jobs, uint32_t njobs,
+                                                           void* stream)
+{
+    if (njobs && !jobs) return kBad;
+    std::vector<Engine::PersistJob> js(njobs);
+    for (uint32_t i = 0; i < njobs; i++) {
+        const xmss_b200_verify_job& j = jobs[i];
+        if (parse(&js[i].p, j.oid, j.mt)) return kBad;
+        if (j.count && (!j.d_pk_index || !j.npk || !j.d_sm || !j.d_sm_off || !j.d_smlen || !j.d_pk || !j.d_status))
+            return kBad;
+        js[i].count = j.count;
+        js[i].d_sm = j.d_sm;
+        js[i].d_sm_off = j.d_sm_off;
+        js[i].d_smlen = j.d_smlen;
+        js[i].d_pk = j.d_pk;
+        js[i].npk = j.npk;
+        js[i].d_pk_index = j.d_pk_index;
+        js[i].d_status = j.d_status;
+    }
+    return guarded([&](Engine& e) {
+        for (auto& j : js) j.ops = xb::ops_for(j.p);
+        cudaStream_t st = (cudaStream_t)stream;
+        e.begin(st);
+        e.verify_persistent_multi(js, st);
+        e.end(st);
+        return kOk;
+    });
+}
+
 extern "C" int xmss_b200_set_wait_bound(unsigned long long ns)
 {
     return guarded([&](Engine& e) {

@@ -467,27 +467,25 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
     XB_CUDA(cudaStreamWaitEvent(st, ss->join, 0));
 }
 
-void Engine::verify_persistent(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_sm,
-                               const uint64_t* d_sm_off, const uint64_t* d_smlen, const uint8_t* d_pk, uint32_t npk,
-                               const uint32_t* d_pk_index, int* d_status, cudaStream_t st)
+void Engine::persist_setup(const PersistJob& j, Workspace& w, VerifyArgs& v, PersistArgs& q, cudaStream_t st)
 {
-    Workspace& w = ws_;
-    XB_CUDA(cudaMemsetAsync(work_, 0, 3 * sizeof(unsigned long long), st));
-    if (!count) return;
+    const FamilyOps* ops = j.ops;
+    const xmss_params& p = j.p;
+    const uint32_t count = j.count, npk = j.npk;
     const uint32_t n = p.n, len = ops->len, d = p.d, nh = len - 1 + p.tree_height;
     const uint32_t groups = (count + 31) / 32;
-    VerifyArgs v{};
-    v.sm = d_sm;
-    v.sm_off = d_sm_off;
-    v.smlen = d_smlen;
-    v.key = d_pk_index;
-    v.key_root = d_pk;
+    v = VerifyArgs{};
+    v.sm = j.d_sm;
+    v.sm_off = j.d_sm_off;
+    v.smlen = j.d_smlen;
+    v.key = j.d_pk_index;
+    v.key_root = j.d_pk;
     v.key_stride = 2 * n;
     v.npk = npk;
     v.node = w.node.as<uint8_t>((size_t)count * n);
     v.lens = w.lens.as<uint8_t>((size_t)count * len);
     v.idx = w.idx.as<uint64_t>(count);
-    v.status = d_status;
+    v.status = j.d_status;
     v.wpk = w.wpk.as<uint8_t>((size_t)count * len * n);
     v.wpk2 = w.wpk2.as<uint8_t>((size_t)count * ((len + 1) / 2) * n);
     v.leaf = w.leaf.as<uint8_t>((size_t)count * n);
@@ -504,7 +502,7 @@ void Engine::verify_persistent(const FamilyOps* ops, const xmss_params& p, uint3
     const size_t words = 4 + gl * 11 + groups;
     uint8_t* st8 = w.pstate.as<uint8_t>(8 + words * 4);
     uint32_t* u = (uint32_t*)(st8 + 8);
-    PersistArgs q{};
+    q = PersistArgs{};
     q.ticket = (unsigned long long*)st8;
     q.hdr = u;
     q.ready = u + 4;
@@ -518,8 +516,94 @@ void Engine::verify_persistent(const FamilyOps* ops, const xmss_params& p, uint3
     q.groups = groups;
     q.wait_ns = persist_wait_ns;
     XB_CUDA(cudaMemsetAsync(st8, 0, 8 + words * 4, st));
+}
+
+void Engine::verify_persistent(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_sm,
+                               const uint64_t* d_sm_off, const uint64_t* d_smlen, const uint8_t* d_pk, uint32_t npk,
+                               const uint32_t* d_pk_index, int* d_status, cudaStream_t st)
+{
+    XB_CUDA(cudaMemsetAsync(work_, 0, 3 * sizeof(unsigned long long), st));
+    if (!count) return;
+    VerifyArgs v;
+    PersistArgs q;
+    persist_setup(PersistJob{ops, p, count, d_sm, d_sm_off, d_smlen, d_pk, npk, d_pk_index, d_status}, ws_, v, q,
+                  st);
     ops->verify_persist(v, q, st);
     XB_CUDA(cudaGetLastError());
+}
+
+void Engine::verify_persistent_multi(const std::vector<PersistJob>& jobs, cudaStream_t st)
+{
+    XB_CUDA(cudaMemsetAsync(work_, 0, 3 * sizeof(unsigned long long), st));
+    // launches: the batches of one family, at most kMaxPersistJobs each
+    std::vector<std::vector<size_t>> launches;
+    std::map<const FamilyOps*, size_t> open;
+    for (size_t i = 0; i < jobs.size(); i++) {
+        if (!jobs[i].count) continue;
+        auto it = open.find(jobs[i].ops);
+        if (it == open.end() || launches[it->second].size() == kMaxPersistJobs) {
+            open[jobs[i].ops] = launches.size();
+            launches.emplace_back();
+        }
+        launches[open[jobs[i].ops]].push_back(i);
+    }
+    if (launches.empty()) return;
+    while (pws_.size() < jobs.size()) pws_.emplace_back(new Workspace());
+    while (pstreams_.size() + 1 < launches.size()) {
+        cudaStream_t s;
+        cudaEvent_t e;
+        XB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        XB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        pstreams_.push_back(s);
+        pjoin_.push_back(e);
+    }
+    if (!pfork_) XB_CUDA(cudaEventCreateWithFlags(&pfork_, cudaEventDisableTiming));
+    // a ticket counter and an exit counter per launch, zeroed before the fork
+    unsigned long long* ctr = pctr_.as<unsigned long long>(2 * launches.size());
+    XB_CUDA(cudaMemsetAsync(ctr, 0, 2 * launches.size() * sizeof(unsigned long long), st));
+    XB_CUDA(cudaEventRecord(pfork_, st));
+    for (size_t l = 0; l < launches.size(); l++) {
+        cudaStream_t s = l == 0 ? st : pstreams_[l - 1];
+        if (l) XB_CUDA(cudaStreamWaitEvent(s, pfork_, 0));
+        PersistJobs P{};
+        P.njobs = (uint32_t)launches[l].size();
+        P.ticket = ctr + 2 * l;
+        P.exited = (uint32_t*)(ctr + 2 * l + 1);
+        uint32_t phases = 0;
+        for (uint32_t k = 0; k < P.njobs; k++) {
+            const size_t i = launches[l][k];
+            persist_setup(jobs[i], *pws_[i], P.v[k], P.q[k], s);
+            phases = std::max(phases, 1 + P.v[k].d);
+        }
+        // segments: phase 0 (contexts, H_msg, h_pre) of every batch, then
+        // each layer of every batch that has it
+        P.nsegs = 0;
+        P.first[0] = 0;
+        for (uint32_t ph = 0; ph < phases; ph++) {
+            for (uint32_t k = 0; k < P.njobs; k++) {
+                const VerifyArgs& v = P.v[k];
+                const PersistArgs& q = P.q[k];
+                if (ph > v.d) continue;
+                const unsigned long long len = jobs[launches[l][k]].ops->len;
+                const unsigned long long G = q.groups, K = (q.npk + 31) / 32;
+                const unsigned long long head = K + G + G * v.d * (len - 1 + v.tree_height);
+                const unsigned long long per_layer = persist_total((int)len, q.groups, q.npk, 1, v.tree_height) -
+                                                     (K + G + G * (len - 1 + v.tree_height));
+                const unsigned long long a = ph == 0 ? 0 : head + (ph - 1) * per_layer;
+                const unsigned long long n = ph == 0 ? head : per_layer;
+                P.job[P.nsegs] = (uint8_t)k;
+                P.local0[P.nsegs] = a;
+                P.first[P.nsegs + 1] = P.first[P.nsegs] + n;
+                P.nsegs++;
+            }
+        }
+        jobs[launches[l][0]].ops->verify_persist_multi(P, s);
+        XB_CUDA(cudaGetLastError());
+        if (l) {
+            XB_CUDA(cudaEventRecord(pjoin_[l - 1], s));
+            XB_CUDA(cudaStreamWaitEvent(st, pjoin_[l - 1], 0));
+        }
+    }
 }
 
 void Engine::last_verify_work(unsigned long long out[3])

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -169,6 +170,24 @@ class Engine {
                            const uint64_t* d_sm_off, const uint64_t* d_smlen, const uint8_t* d_pk, uint32_t npk,
                            const uint32_t* d_pk_index, int* d_status, cudaStream_t st);
 
+    // One verify batch of the persistent form (device pointers).
+    struct PersistJob {
+        const FamilyOps* ops;
+        xmss_params p;
+        uint32_t count;
+        const uint8_t* d_sm;
+        const uint64_t* d_sm_off;
+        const uint64_t* d_smlen;
+        const uint8_t* d_pk;
+        uint32_t npk;
+        const uint32_t* d_pk_index;
+        int* d_status;
+    };
+    // Batches of any parameter sets: one persistent launch per hash family
+    // (up to 8 batches each), the families' launches on streams forked from
+    // st and joined back into it.
+    void verify_persistent_multi(const std::vector<PersistJob>& jobs, cudaStream_t st);
+
     // Key generation from seeds (count x 3n) into pk (count x 2n) and sk
     // (count x sk_bytes), no OID prefix.
     void keypair(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* d_seeds, uint8_t* d_pk,
@@ -242,6 +261,14 @@ class Engine {
     Workspace ws_;  // scratch of the engine's own entry points
     DevBuf s_work_;
     unsigned long long* work_ = nullptr;
+    // persistent batches: arguments of one batch over workspace w, its task
+    // counters zeroed on st
+    void persist_setup(const PersistJob& j, Workspace& w, VerifyArgs& v, PersistArgs& q, cudaStream_t st);
+    std::vector<std::unique_ptr<Workspace>> pws_;  // one per batch of a multi-batch launch
+    DevBuf pctr_;                                  // ticket and exit counters of those launches
+    std::vector<cudaStream_t> pstreams_;           // launches after the first
+    std::vector<cudaEvent_t> pjoin_;
+    cudaEvent_t pfork_ = nullptr;
     struct Mark {
         int phase;
         cudaEvent_t a, b;

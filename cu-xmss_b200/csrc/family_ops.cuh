@@ -190,6 +190,18 @@ struct Launch {
         }();
         k_verify_persist<F, FT><<<grid, 128, 0, st>>>(v, q);
     }
+    static void verify_persist_multi(const PersistJobs& P, cudaStream_t st)
+    {
+        if (!P.njobs) return;
+        static const unsigned grid = [] {
+            int dev = 0, sms = 0, per = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_verify_persist_multi<F, FT>, 128, 0);
+            return (unsigned)(sms * (per > 0 ? per : 1));
+        }();
+        k_verify_persist_multi<F, FT><<<grid, 128, 0, st>>>(P);
+    }
     static void sign_prep(const SignArgs& g, const void* ctx, cudaStream_t st)
     {
         if (!g.count) return;
@@ -238,6 +250,7 @@ struct Launch {
         o.verify_root = verify_root;
         o.verify_ltree_warp = verify_ltree_warp;
         o.verify_persist = verify_persist;
+        o.verify_persist_multi = verify_persist_multi;
         o.sign_prep = sign_prep;
         o.sign_chains = sign_chains;
         o.core_hash = core_hash;

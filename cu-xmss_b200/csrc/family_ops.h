@@ -14,6 +14,7 @@ struct TreeJob;
 struct VerifyArgs;
 struct SignArgs;
 struct PersistArgs;
+struct PersistJobs;
 
 struct FamilyOps {
     const char* name;
@@ -45,6 +46,8 @@ struct FamilyOps {
     void (*verify_ltree_warp)(const VerifyArgs& v, uint32_t layer, cudaStream_t st);  // whole L-tree, warp / sig
     // the whole verify (every layer) as one persistent launch (verify_persist.cuh)
     void (*verify_persist)(const VerifyArgs& v, const PersistArgs& q, cudaStream_t st);
+    // several batches of this family's parameter sets as one persistent launch
+    void (*verify_persist_multi)(const PersistJobs& jobs, cudaStream_t st);
     void (*sign_prep)(const SignArgs& g, const void* ctx, cudaStream_t st);
     void (*sign_chains)(const SignArgs& g, const void* ctx, cudaStream_t st);
     void (*core_hash)(const uint8_t* msgs, const uint64_t* off, const uint64_t* len, uint32_t count, uint8_t* out,

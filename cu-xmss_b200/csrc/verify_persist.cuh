@@ -220,18 +220,33 @@ constexpr int persist_min_ctas()
     return HMsgKind<F>::v == 0 ? 5 : 2;
 }
 
-// F runs every task except the chains, which run FT (same family, another
-// pipe mix; the key context is shared).
+// Tickets of one batch: key contexts, H_msg groups, h_pre items, then per
+// layer the chain, L-tree and root tasks.
+__host__ __device__ inline unsigned long long persist_total(int len, uint32_t groups, uint32_t npk, uint32_t d,
+                                                            uint32_t th)
+{
+    const unsigned long long G = groups, K = (npk + 31) / 32;
+    const unsigned long long n_hpre = G * d * (len - 1 + th);
+    return K + G + n_hpre + G * (len + lt_items_total(len) + 1) * d;
+}
+template <class F>
+__device__ __forceinline__ unsigned long long persist_tickets(const VerifyArgs& v, const PersistArgs& q)
+{
+    return persist_total(F::LEN, q.groups, q.npk, v.d, v.tree_height);
+}
+
+// Runs ticket t of one batch (whole warp).  F runs every task except the
+// chains, which run FT (same family, another pipe mix; the key context is
+// shared).  cnt: 32 words of this warp's shared memory.  False when a
+// dependency wait ran out or the batch failed.
 template <class F, class FT>
-__global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(VerifyArgs v, PersistArgs q)
+__device__ __forceinline__ bool persist_step(const VerifyArgs& v, const PersistArgs& q, unsigned long long t,
+                                             uint32_t* cnt)
 {
     using Ctx = typename F::Ctx;
     using HPre = typename F::HPre;
     constexpr int LEN = F::LEN, LV = lt_levels(F::LEN), LT = lt_items_total(F::LEN);
-    __shared__ uint32_t sh_cnt[4][32];
-    __shared__ int sh_last;
     const uint32_t lane = threadIdx.x & 31;
-    uint32_t* cnt = sh_cnt[(threadIdx.x >> 5) & 3];
     uint32_t* err = q.hdr;
     Ctx* ctx = (Ctx*)q.ctx;
     const uint32_t G = q.groups, d = v.d, th = v.tree_height;
@@ -239,180 +254,194 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
     const unsigned long long K = (q.npk + 31) / 32;
     const unsigned long long n_hpre = (unsigned long long)G * d * nh;
     const unsigned long long per_layer = (unsigned long long)G * (LEN + LT + 1);
-    const unsigned long long total = K + G + n_hpre + per_layer * d;
 
+    if (t < K) {  // -------- ctx: 32 keys
+        const uint32_t k = (uint32_t)t * 32 + lane;
+        if (k < q.npk) {
+            Ctx c;
+            F::make_ctx(c, v.key_root + (uint64_t)k * v.key_stride + F::N, nullptr, nullptr);
+            ctx[k] = c;
+        }
+        persist_signal(&q.hdr[2]);
+        return true;
+    }
+    t -= K;
+    if (t < G) {  // -------- H_msg + base_w of one group, then its layer-0 list
+        const uint32_t g = (uint32_t)t, s = g * 32 + lane;
+        bool live = false;
+        if (s < v.count) {
+            const uint64_t smlen = v.smlen[s];
+            if (!verify_input_ok(v, s)) {  // too short, or a key index outside the table
+                v.status[s] = -1;
+            } else {
+                const uint8_t* sm = v.sm + v.sm_off[s];
+                const uint64_t idx = bytes_be(sm, (int)v.index_bytes);
+                uint32_t R[F::NW], root[F::NW], mh[F::NW];
+                F::load(R, sm + v.index_bytes);
+                F::load(root, v.key_root + (uint64_t)v.key[s] * v.key_stride);
+                hmsg<F>(mh, R, root, idx, sm + v.sig_bytes, smlen - v.sig_bytes);
+                F::store(v.node + (uint64_t)s * F::N, mh);
+                chain_lengths<F>(v.lens + (uint64_t)s * F::LEN, mh);
+                v.idx[s] = idx;
+                v.status[s] = 0;
+                live = true;
+                if (v.work) {
+                    atomicAdd(&v.work[0], hmsg_blocks<F>(smlen - v.sig_bytes));
+                    atomicAdd(&v.work[2], (unsigned long long)nh * d);
+                }
+            }
+        }
+        persist_bucket<F>(v, q, g, 0, live, s, cnt);
+        return true;
+    }
+    t -= G;
+    if (t < n_hpre) {  // -------- h_pre of one H node of one layer, for a group
+        const uint32_t g = (uint32_t)(t / ((unsigned long long)d * nh));
+        const uint32_t k = (uint32_t)(t - (unsigned long long)g * d * nh);
+        if (!persist_wait(&q.hdr[2], (uint32_t)K, err, q.wait_ns)) return false;
+        const uint32_t s = g * 32 + lane;
+        if (s < v.count) verify_hpre_item<F>(v, ctx, (uint64_t)s * d * nh + k);
+        persist_signal(&q.hpre_done[g]);
+        return true;
+    }
+    t -= n_hpre;
+    const uint32_t layer = (uint32_t)(t / per_layer);
+    unsigned long long r = t - (unsigned long long)layer * per_layer;
+    uint32_t leafidx;
+    uint64_t tree;
+    if (r < (unsigned long long)G * LEN) {  // -------- 32 chains of a group's list
+        const uint32_t c = (uint32_t)(r / G), g = (uint32_t)(r - (unsigned long long)c * G);
+        const uint32_t gl = g * d + layer;
+        if (!persist_wait(&q.ready[gl], 1u, err, q.wait_ns)) return false;
+        if (layer == 0 && !persist_wait(&q.hdr[2], (uint32_t)K, err, q.wait_ns)) return false;
+        const uint32_t e = c * 32 + lane;
+        if (e < q.ntot[gl]) {
+            const uint32_t item = q.list[(uint64_t)g * 32 * LEN + e];
+            const uint32_t s = item / LEN, chain = item - s * LEN;
+            layer_addr<F>(v.idx[s], th, layer, leafidx, tree);
+            const uint32_t start = v.lens[item];
+            const uint64_t wsb = (uint64_t)LEN * F::N;
+            const uint8_t* sig = v.sm + v.sm_off[s] + v.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N);
+            uint32_t x[F::NW], a[8];
+            F::load(x, sig + (uint64_t)chain * F::N);
+            set_addr(a, layer, tree, ADDR_OTS, leafidx, chain, 0);
+            // the key context in registers: ctx is written by this launch, so
+            // the chain loop cannot read it through the read-only path, and
+            // re-reading its midstate from L1 / L2 on every F call made a
+            // lone chain warp ~3x slower than in k_verify_chains
+            const typename FT::Ctx kc = ((const typename FT::Ctx*)ctx)[v.key[s]];
+            run_chain<FT>(x, kc, a, start, 15 - start, false);
+            F::store(v.wpk + (uint64_t)item * F::N, x);
+        }
+        persist_signal(&q.chains_done[gl]);
+        return true;
+    }
+    r -= (unsigned long long)G * LEN;
+    if (r < (unsigned long long)G * LT) {  // -------- one pair index of one L-tree level
+        int lev = 0;
+        while (r >= (unsigned long long)G * lt_items(LEN, lev)) {
+            r -= (unsigned long long)G * lt_items(LEN, lev);
+            lev++;
+        }
+        const uint32_t items = (uint32_t)lt_items(LEN, lev);
+        const uint32_t g = (uint32_t)(r / items), p = (uint32_t)(r - (unsigned long long)g * items);
+        const uint32_t gl = g * d + layer;
+        if (lev == 0) {
+            if (!persist_wait(&q.chains_done[gl], (uint32_t)LEN, err, q.wait_ns)) return false;
+            if (!persist_wait(&q.hpre_done[g], d * nh, err, q.wait_ns)) return false;
+        } else if (!persist_wait(&q.lt_done[gl * 8 + lev - 1], (uint32_t)lt_items(LEN, lev - 1), err, q.wait_ns)) {
+            return false;
+        }
+        const uint32_t s = g * 32 + lane;
+        if (s < v.count && v.status[s] == 0) {
+            const int cin = lt_cnt(LEN, lev);
+            // levels alternate between the WOTS pk buffer and the half-size one
+            const bool even = (lev & 1) == 0;
+            const uint8_t* src = even ? v.wpk + (uint64_t)s * LEN * F::N : v.wpk2 + (uint64_t)s * ((LEN + 1) / 2) * F::N;
+            uint8_t* out = (cin == 2) ? v.leaf + (uint64_t)s * F::N
+                           : even     ? v.wpk2 + ((uint64_t)s * ((LEN + 1) / 2) + p) * F::N
+                                      : v.wpk + ((uint64_t)s * LEN + p) * F::N;
+            uint32_t l[F::NW], o[F::NW];
+            F::load(l, src + (uint64_t)(2 * p) * F::N);
+            if (2 * (int)p + 1 < cin) {
+                uint32_t rr[F::NW];
+                F::load(rr, src + (uint64_t)(2 * p + 1) * F::N);
+                const HPre& hp = ((const HPre*)v.hpre)[((uint64_t)s * d + layer) * nh + lt_base(LEN, lev) + p];
+                F::h_fin(o, hp, l, rr);
+                F::store(out, o);
+            } else {
+                F::store(out, l);
+            }
+        }
+        persist_signal(&q.lt_done[gl * 8 + lev]);
+        return true;
+    }
+    r -= (unsigned long long)G * LT;
+    {  // -------- compute_root of a group, then the next layer's list or the verdict
+        const uint32_t g = (uint32_t)r, gl = g * d + layer;
+        if (!persist_wait(&q.lt_done[gl * 8 + LV - 1], 1u, err, q.wait_ns)) return false;
+        const uint32_t s = g * 32 + lane;
+        const bool live = s < v.count && v.status[s] == 0;
+        bool next_live = false;
+        if (live) {
+            layer_addr<F>(v.idx[s], th, layer, leafidx, tree);
+            const uint64_t wsb = (uint64_t)LEN * F::N;
+            const uint8_t* auth =
+                v.sm + v.sm_off[s] + v.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N) + wsb;
+            const HPre* hp = (const HPre*)v.hpre + ((uint64_t)s * d + layer) * nh + (LEN - 1);
+            uint32_t cur[F::NW], sib[F::NW];
+            F::load(cur, v.leaf + (uint64_t)s * F::N);
+#pragma unroll 1
+            for (uint32_t i = 0; i < th; i++) {
+                F::load(sib, auth + (uint64_t)i * F::N);
+                // the node goes right when its index is odd (xmss_commons.c:61-69)
+                const bool odd = leafidx & 1;
+                uint32_t l[F::NW], rr[F::NW];
+#pragma unroll
+                for (int k = 0; k < F::NW; k++) {
+                    l[k] = odd ? sib[k] : cur[k];
+                    rr[k] = odd ? cur[k] : sib[k];
+                }
+                F::h_fin(cur, hp[i], l, rr);
+                leafidx >>= 1;
+            }
+            if (layer + 1 < d) {
+                F::store(v.node + (uint64_t)s * F::N, cur);
+                chain_lengths<F>(v.lens + (uint64_t)s * F::LEN, cur);
+                next_live = true;
+            } else {
+                uint32_t pr[F::NW];
+                F::load(pr, v.key_root + (uint64_t)v.key[s] * v.key_stride);
+                uint32_t diff = 0;
+#pragma unroll
+                for (int i = 0; i < F::NW; i++) diff |= pr[i] ^ cur[i];
+                v.status[s] = diff ? -1 : 0;
+            }
+        }
+        if (layer + 1 < d) persist_bucket<F>(v, q, g, layer + 1, next_live, s, cnt);
+        return true;
+    }
+    return true;
+}
+
+// One batch in one launch: warps pop tickets from q.ticket until the
+// sequence is exhausted.
+template <class F, class FT>
+__global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(const __grid_constant__ VerifyArgs v,
+                                                                              const __grid_constant__ PersistArgs q)
+{
+    __shared__ uint32_t sh_cnt[4][32];
+    __shared__ int sh_last;
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t* cnt = sh_cnt[(threadIdx.x >> 5) & 3];
+    uint32_t* err = q.hdr;
+    const unsigned long long total = persist_tickets<F>(v, q);
     for (;;) {
         unsigned long long t = 0;
         if (lane == 0) t = atomicAdd(q.ticket, 1ull);
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= total || *(volatile uint32_t*)err) break;
-
-        if (t < K) {  // -------- ctx: 32 keys
-            const uint32_t k = (uint32_t)t * 32 + lane;
-            if (k < q.npk) {
-                Ctx c;
-                F::make_ctx(c, v.key_root + (uint64_t)k * v.key_stride + F::N, nullptr, nullptr);
-                ctx[k] = c;
-            }
-            persist_signal(&q.hdr[2]);
-            continue;
-        }
-        t -= K;
-        if (t < G) {  // -------- H_msg + base_w of one group, then its layer-0 list
-            const uint32_t g = (uint32_t)t, s = g * 32 + lane;
-            bool live = false;
-            if (s < v.count) {
-                const uint64_t smlen = v.smlen[s];
-                if (!verify_input_ok(v, s)) {  // too short, or a key index outside the table
-                    v.status[s] = -1;
-                } else {
-                    const uint8_t* sm = v.sm + v.sm_off[s];
-                    const uint64_t idx = bytes_be(sm, (int)v.index_bytes);
-                    uint32_t R[F::NW], root[F::NW], mh[F::NW];
-                    F::load(R, sm + v.index_bytes);
-                    F::load(root, v.key_root + (uint64_t)v.key[s] * v.key_stride);
-                    hmsg<F>(mh, R, root, idx, sm + v.sig_bytes, smlen - v.sig_bytes);
-                    F::store(v.node + (uint64_t)s * F::N, mh);
-                    chain_lengths<F>(v.lens + (uint64_t)s * F::LEN, mh);
-                    v.idx[s] = idx;
-                    v.status[s] = 0;
-                    live = true;
-                    if (v.work) {
-                        atomicAdd(&v.work[0], hmsg_blocks<F>(smlen - v.sig_bytes));
-                        atomicAdd(&v.work[2], (unsigned long long)nh * d);
-                    }
-                }
-            }
-            persist_bucket<F>(v, q, g, 0, live, s, cnt);
-            continue;
-        }
-        t -= G;
-        if (t < n_hpre) {  // -------- h_pre of one H node of one layer, for a group
-            const uint32_t g = (uint32_t)(t / ((unsigned long long)d * nh));
-            const uint32_t k = (uint32_t)(t - (unsigned long long)g * d * nh);
-            if (!persist_wait(&q.hdr[2], (uint32_t)K, err, q.wait_ns)) break;
-            const uint32_t s = g * 32 + lane;
-            if (s < v.count) verify_hpre_item<F>(v, ctx, (uint64_t)s * d * nh + k);
-            persist_signal(&q.hpre_done[g]);
-            continue;
-        }
-        t -= n_hpre;
-        const uint32_t layer = (uint32_t)(t / per_layer);
-        unsigned long long r = t - (unsigned long long)layer * per_layer;
-        uint32_t leafidx;
-        uint64_t tree;
-        if (r < (unsigned long long)G * LEN) {  // -------- 32 chains of a group's list
-            const uint32_t c = (uint32_t)(r / G), g = (uint32_t)(r - (unsigned long long)c * G);
-            const uint32_t gl = g * d + layer;
-            if (!persist_wait(&q.ready[gl], 1u, err, q.wait_ns)) break;
-            if (layer == 0 && !persist_wait(&q.hdr[2], (uint32_t)K, err, q.wait_ns)) break;
-            const uint32_t e = c * 32 + lane;
-            if (e < q.ntot[gl]) {
-                const uint32_t item = q.list[(uint64_t)g * 32 * LEN + e];
-                const uint32_t s = item / LEN, chain = item - s * LEN;
-                layer_addr<F>(v.idx[s], th, layer, leafidx, tree);
-                const uint32_t start = v.lens[item];
-                const uint64_t wsb = (uint64_t)LEN * F::N;
-                const uint8_t* sig = v.sm + v.sm_off[s] + v.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N);
-                uint32_t x[F::NW], a[8];
-                F::load(x, sig + (uint64_t)chain * F::N);
-                set_addr(a, layer, tree, ADDR_OTS, leafidx, chain, 0);
-                // the key context in registers: ctx is written by this launch, so
-                // the chain loop cannot read it through the read-only path, and
-                // re-reading its midstate from L1 / L2 on every F call made a
-                // lone chain warp ~3x slower than in k_verify_chains
-                const typename FT::Ctx kc = ((const typename FT::Ctx*)ctx)[v.key[s]];
-                run_chain<FT>(x, kc, a, start, 15 - start, false);
-                F::store(v.wpk + (uint64_t)item * F::N, x);
-            }
-            persist_signal(&q.chains_done[gl]);
-            continue;
-        }
-        r -= (unsigned long long)G * LEN;
-        if (r < (unsigned long long)G * LT) {  // -------- one pair index of one L-tree level
-            int lev = 0;
-            while (r >= (unsigned long long)G * lt_items(LEN, lev)) {
-                r -= (unsigned long long)G * lt_items(LEN, lev);
-                lev++;
-            }
-            const uint32_t items = (uint32_t)lt_items(LEN, lev);
-            const uint32_t g = (uint32_t)(r / items), p = (uint32_t)(r - (unsigned long long)g * items);
-            const uint32_t gl = g * d + layer;
-            if (lev == 0) {
-                if (!persist_wait(&q.chains_done[gl], (uint32_t)LEN, err, q.wait_ns)) break;
-                if (!persist_wait(&q.hpre_done[g], d * nh, err, q.wait_ns)) break;
-            } else if (!persist_wait(&q.lt_done[gl * 8 + lev - 1], (uint32_t)lt_items(LEN, lev - 1), err, q.wait_ns)) {
-                break;
-            }
-            const uint32_t s = g * 32 + lane;
-            if (s < v.count && v.status[s] == 0) {
-                const int cin = lt_cnt(LEN, lev);
-                // levels alternate between the WOTS pk buffer and the half-size one
-                const bool even = (lev & 1) == 0;
-                const uint8_t* src = even ? v.wpk + (uint64_t)s * LEN * F::N : v.wpk2 + (uint64_t)s * ((LEN + 1) / 2) * F::N;
-                uint8_t* out = (cin == 2) ? v.leaf + (uint64_t)s * F::N
-                               : even     ? v.wpk2 + ((uint64_t)s * ((LEN + 1) / 2) + p) * F::N
-                                          : v.wpk + ((uint64_t)s * LEN + p) * F::N;
-                uint32_t l[F::NW], o[F::NW];
-                F::load(l, src + (uint64_t)(2 * p) * F::N);
-                if (2 * (int)p + 1 < cin) {
-                    uint32_t rr[F::NW];
-                    F::load(rr, src + (uint64_t)(2 * p + 1) * F::N);
-                    const HPre& hp = ((const HPre*)v.hpre)[((uint64_t)s * d + layer) * nh + lt_base(LEN, lev) + p];
-                    F::h_fin(o, hp, l, rr);
-                    F::store(out, o);
-                } else {
-                    F::store(out, l);
-                }
-            }
-            persist_signal(&q.lt_done[gl * 8 + lev]);
-            continue;
-        }
-        r -= (unsigned long long)G * LT;
-        {  // -------- compute_root of a group, then the next layer's list or the verdict
-            const uint32_t g = (uint32_t)r, gl = g * d + layer;
-            if (!persist_wait(&q.lt_done[gl * 8 + LV - 1], 1u, err, q.wait_ns)) break;
-            const uint32_t s = g * 32 + lane;
-            const bool live = s < v.count && v.status[s] == 0;
-            bool next_live = false;
-            if (live) {
-                layer_addr<F>(v.idx[s], th, layer, leafidx, tree);
-                const uint64_t wsb = (uint64_t)LEN * F::N;
-                const uint8_t* auth =
-                    v.sm + v.sm_off[s] + v.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N) + wsb;
-                const HPre* hp = (const HPre*)v.hpre + ((uint64_t)s * d + layer) * nh + (LEN - 1);
-                uint32_t cur[F::NW], sib[F::NW];
-                F::load(cur, v.leaf + (uint64_t)s * F::N);
-#pragma unroll 1
-                for (uint32_t i = 0; i < th; i++) {
-                    F::load(sib, auth + (uint64_t)i * F::N);
-                    // the node goes right when its index is odd (xmss_commons.c:61-69)
-                    const bool odd = leafidx & 1;
-                    uint32_t l[F::NW], rr[F::NW];
-#pragma unroll
-                    for (int k = 0; k < F::NW; k++) {
-                        l[k] = odd ? sib[k] : cur[k];
-                        rr[k] = odd ? cur[k] : sib[k];
-                    }
-                    F::h_fin(cur, hp[i], l, rr);
-                    leafidx >>= 1;
-                }
-                if (layer + 1 < d) {
-                    F::store(v.node + (uint64_t)s * F::N, cur);
-                    chain_lengths<F>(v.lens + (uint64_t)s * F::LEN, cur);
-                    next_live = true;
-                } else {
-                    uint32_t pr[F::NW];
-                    F::load(pr, v.key_root + (uint64_t)v.key[s] * v.key_stride);
-                    uint32_t diff = 0;
-#pragma unroll
-                    for (int i = 0; i < F::NW; i++) diff |= pr[i] ^ cur[i];
-                    v.status[s] = diff ? -1 : 0;
-                }
-            }
-            if (layer + 1 < d) persist_bucket<F>(v, q, g, layer + 1, next_live, s, cnt);
-            continue;
-        }
+        if (!persist_step<F, FT>(v, q, t, cnt)) break;
     }
 
     // The last CTA out turns a failed launch into -3 for every signature.
@@ -426,6 +455,65 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(V
         __threadfence();
         if (*(volatile uint32_t*)err)
             for (uint32_t s = threadIdx.x; s < v.count; s += blockDim.x) v.status[s] = -3;
+    }
+}
+
+// Batches of several parameter sets of one family (same F: LEN and n
+// agree, d, h', index and signature sizes may differ) in ONE launch over one
+// shared ticket counter.  Each batch's ticket sequence is cut into phases -
+// its key contexts, H_msg and h_pre, then one phase per layer - and the
+// shared sequence takes phase 0 of every batch, then layer 0 of every batch,
+// then layer 1 of the batches that have one, and so on (segment s = local
+// tickets [local0[s], local0[s] + first[s + 1] - first[s]) of batch job[s]).
+// Every batch keeps its own order and depends on nothing of the others, so
+// the sequence is still topological and the launch completes whatever the
+// residency, while the batches run their phases side by side.  A batch whose
+// dependency wait ran out (its own error flag) skips its remaining tickets
+// and ends with -3 in its statuses; the others finish.
+constexpr uint32_t kMaxPersistJobs = 8;
+constexpr uint32_t kMaxPersistSegs = kMaxPersistJobs * 13;  // phases: 1 + up to 12 layers
+struct PersistJobs {
+    VerifyArgs v[kMaxPersistJobs];
+    PersistArgs q[kMaxPersistJobs];
+    unsigned long long first[kMaxPersistSegs + 1];  // first shared ticket of each segment
+    unsigned long long local0[kMaxPersistSegs];     // its first ticket in its batch's sequence
+    uint8_t job[kMaxPersistSegs];                   // its batch
+    unsigned long long* ticket;  // the shared ticket counter (zeroed before the launch)
+    uint32_t* exited;            // CTAs that have left the loop (zeroed before the launch)
+    uint32_t njobs, nsegs;
+};
+
+template <class F, class FT>
+__global__ void __launch_bounds__(128, persist_min_ctas<F>())
+    k_verify_persist_multi(const __grid_constant__ PersistJobs P)
+{
+    __shared__ uint32_t sh_cnt[4][32];
+    __shared__ int sh_last;
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t* cnt = sh_cnt[(threadIdx.x >> 5) & 3];
+    const unsigned long long total = P.first[P.nsegs];
+    uint32_t sg = 0;  // a warp's tickets only grow, so its segment only grows
+    for (;;) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(P.ticket, 1ull);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= total) break;
+        while (t >= P.first[sg + 1]) sg++;
+        const uint32_t j = P.job[sg];
+        if (*(volatile uint32_t*)P.q[j].hdr) continue;  // that batch failed
+        persist_step<F, FT>(P.v[j], P.q[j], P.local0[sg] + (t - P.first[sg]), cnt);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        sh_last = atomicAdd(P.exited, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (sh_last) {
+        __threadfence();
+        for (uint32_t k = 0; k < P.njobs; k++)
+            if (*(volatile uint32_t*)P.q[k].hdr)
+                for (uint32_t s = threadIdx.x; s < P.v[k].count; s += blockDim.x) P.v[k].status[s] = -3;
     }
 }
 

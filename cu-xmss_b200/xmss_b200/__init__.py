@@ -558,6 +558,29 @@ def sign_open_device_persistent(oid: int, mt: bool, count: int, d_sm: int, d_sm_
         raise ValueError(f"sign_open_device_persistent returned {r}: {last_error()}")
 
 
+class VerifyJob(C.Structure):
+    """xmss_b200_verify_job (include/xmss_b200.h); d_ fields are device pointers as ints."""
+    _fields_ = [("oid", C.c_uint32), ("mt", C.c_int), ("count", C.c_uint32), ("d_sm", C.c_void_p),
+                ("d_sm_off", C.c_void_p), ("d_smlen", C.c_void_p), ("d_pk", C.c_void_p), ("npk", C.c_uint32),
+                ("d_pk_index", C.c_void_p), ("d_status", C.c_void_p)]
+
+
+lib.xmss_b200_sign_open_device_persistent_multi.argtypes = [C.POINTER(VerifyJob), C.c_uint32, C.c_void_p]
+
+
+def sign_open_device_persistent_multi(jobs: Sequence[dict], stream: int = 0) -> None:
+    """xmss_b200_sign_open_device_persistent_multi: batches of any parameter
+    sets, one persistent launch per hash family (jobs: dicts of VerifyJob fields)."""
+    arr = (VerifyJob * len(jobs))()
+    for i, j in enumerate(jobs):
+        for k, v in j.items():
+            setattr(arr[i], k, int(v))
+    r = _check(lib.xmss_b200_sign_open_device_persistent_multi(arr, len(jobs), stream),
+               "sign_open_device_persistent_multi")
+    if r:
+        raise ValueError(f"sign_open_device_persistent_multi returned {r}: {last_error()}")
+
+
 def set_wait_bound(ns: int) -> None:
     """xmss_b200_set_wait_bound: bound of one dependency wait inside later
     persistent launches, in ns (0 = the default of 8 s)."""

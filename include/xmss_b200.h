@@ -83,6 +83,31 @@ int xmss_b200_sign_open_device_persistent(uint32_t oid, int mt, uint32_t count, 
                                           const uint8_t *d_pk, uint32_t npk, const uint32_t *d_pk_index,
                                           int *d_status, void *stream);
 
+/* Persistent form over several batches of ANY parameter sets (XMSS and
+ * XMSS^MT, every family): the batches of one hash family run as ONE
+ * persistent launch (up to 8 batches per launch; each batch's tickets
+ * follow the previous batch's in one shared ticket sequence, so the next
+ * batch's work fills the SMs during one batch's serial tail), and the
+ * families' launches run concurrently on streams forked from `stream` and
+ * joined back into it (capturable in a CUDA graph).  Each batch gets the
+ * statuses of xmss_b200_sign_open_device; a batch whose dependency wait runs
+ * out gets -3 in every status, the others finish.  Asynchronous on stream;
+ * 0 ok, -1 bad job (unknown OID, missing pointer), -3 GPU failure. */
+typedef struct {
+    uint32_t oid;
+    int mt;
+    uint32_t count;
+    const uint8_t *d_sm;
+    const uint64_t *d_sm_off;
+    const uint64_t *d_smlen;
+    const uint8_t *d_pk;         /* npk x 2n (root || PUB_SEED) */
+    uint32_t npk;
+    const uint32_t *d_pk_index;
+    int *d_status;
+} xmss_b200_verify_job;
+
+int xmss_b200_sign_open_device_persistent_multi(const xmss_b200_verify_job *jobs, uint32_t njobs, void *stream);
+
 /* Bound of one dependency wait inside a persistent launch, in ns of the
  * GPU's global timer;
  * 0 restores the default of 8 s.  A wait that runs out ends the launch with

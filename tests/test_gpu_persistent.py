@@ -116,3 +116,44 @@ def test_persistent_large_batch_last_index(xb):
     got = _device_statuses(xb, torch, xb.sign_open_device_persistent, 1, False, buf, off, ln, pks, keyix, calls=2)
     for g in got:
         assert (g == expect).all()
+
+
+def test_persistent_multi_mixed_sets(xb):
+    """xmss_b200_sign_open_device_persistent_multi: batches of five parameter
+    sets (four SHA-256 n = 32 sets in one persistent launch, XMSS-SHAKE_10_256
+    in a second launch on a forked stream) give every batch the statuses its
+    own multi-launch verify gives, twice in a row (counters restart), and a
+    set of nine SHA-256 batches (more than one launch of a family) as well."""
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    names = ["XMSS-SHA2_10_256", "XMSSMT-SHA2_20/2_256", "XMSSMT-SHA2_20/4_256", "XMSSMT-SHA2_40/4_256",
+             "XMSS-SHAKE_10_256"]
+    batches = [_signed_batch(xb, nm, c, seed=100 + i) for i, (nm, c) in enumerate(zip(names, (90, 70, 40, 33, 50)))]
+    keep, jobs, want = [], [], []
+    for oid, mt, buf, off, ln, pks, keyix, expect in batches:
+        d = dict(d_sm=torch.from_numpy(buf).to(dev), d_sm_off=torch.from_numpy(off.astype(np.int64)).to(dev),
+                 d_smlen=torch.from_numpy(ln.astype(np.int64)).to(dev),
+                 d_pk=torch.from_numpy(np.ascontiguousarray(pks[:, 4:])).to(dev),
+                 d_pk_index=torch.from_numpy(keyix.astype(np.int32)).to(dev),
+                 d_status=torch.full((len(off),), 7, dtype=torch.int32, device=dev))
+        keep.append(d)
+        jobs.append(dict(oid=oid, mt=int(mt), count=len(off), npk=len(pks),
+                         **{k: v.data_ptr() for k, v in d.items()}))
+        ref = _device_statuses(xb, torch, xb.sign_open_device, oid, mt, buf, off, ln, pks, keyix)[0]
+        assert (ref == expect).all()
+        want.append(ref)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    for _ in range(2):
+        for d in keep:
+            d["d_status"].fill_(7)
+        xb.sign_open_device_persistent_multi(jobs, stream)
+        torch.cuda.synchronize()
+        for d, w, nm in zip(keep, want, names):
+            assert (d["d_status"].cpu().numpy() == w).all(), nm
+    # nine batches of one family (two launches of it), each with its own statuses
+    st9 = [torch.full((jobs[i % 4]["count"],), 7, dtype=torch.int32, device=dev) for i in range(9)]
+    jobs9 = [dict(jobs[i % 4], d_status=st9[i].data_ptr()) for i in range(9)]
+    xb.sign_open_device_persistent_multi(jobs9, stream)
+    torch.cuda.synchronize()
+    for i in range(9):
+        assert (st9[i].cpu().numpy() == want[i % 4]).all(), (i, names[i % 4])
