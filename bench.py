@@ -967,7 +967,10 @@ def _batch_inputs(xb, torch, dev, rng):
         groups.append(dict(kind=xb.VERIFY, oid=oid, mt=int(mt), count=count, d_sm=d_sm.data_ptr(),
                            d_sm_off=d_off.data_ptr(), d_len=d_len.data_ptr(), d_pk=d_pk.data_ptr(), npk=nkeys,
                            d_pk_index=d_kix.data_ptr(), d_status=d_st.data_ptr()))
-        expect.append(("verify", want, d_st))
+        expect.append(("verify", want, d_st, dict(oid=oid, mt=int(mt), count=count, d_sm=d_sm.data_ptr(),
+                                                  d_sm_off=d_off.data_ptr(), d_smlen=d_len.data_ptr(),
+                                                  d_pk=d_pk.data_ptr(), npk=nkeys, d_pk_index=d_kix.data_ptr(),
+                                                  d_status=d_st.data_ptr())))
     return groups, expect, keep
 
 
@@ -1021,12 +1024,41 @@ def batch_rates(xb, torch, dev, sh, repeats: int = 5):
             ok &= all(sm[int(o):int(o) + len(w)].tobytes() == w for w, o in zip(e[1], e[2]))
         else:
             ok &= bool((e[2].cpu().numpy() == e[1]).all())
+    # the verify groups alone: one persistent launch per family over the
+    # mixed sets, against each set's multi-launch verify in turn
+    jobs = [e[3] for e in expect if e[0] == "verify"]
+    vstat = [e for e in expect if e[0] == "verify"]
+
+    def each():
+        for j in jobs:
+            xb.sign_open_device(j["oid"], bool(j["mt"]), j["count"], j["d_sm"], j["d_sm_off"], j["d_smlen"], j["d_pk"],
+                                j["npk"], j["d_pk_index"], j["d_status"], sh)
+
+    def multi():
+        xb.sign_open_device_persistent_multi(jobs, sh)
+
+    vt = {}
+    for name, f in (("multi_launch_each_set", each), ("persistent_one_launch_per_family", multi)):
+        f()
+        ts = []
+        for _ in range(repeats):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            f()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        vt[name] = float(np.median(ts))
+        ok &= all(bool((e[2].cpu().numpy() == e[1]).all()) for e in vstat)
     items = sum(g[3] for g in BATCH_GROUPS)
     ms, ms_seq = float(np.median(one)), float(np.median(seq))
     out = {"workload": "mixed batch, one CUDA graph",
            "groups": [{"kind": k, "set": nm, "items": c} for k, nm, _, c, _ in BATCH_GROUPS],
            "items": items, "ms_per_batch": ms, "items_per_s": items / (ms / 1e3),
            "ms_groups_one_graph_each_back_to_back": ms_seq, "repeats": repeats,
+           "verify_groups_ms": vt,
            "correct": bool(ok), "check": "every key, signature and status equal to the per-kind entry points "
                                         "(keypair_batch, sign_batch, expected accept bitmap)"}
     log(out)
