@@ -182,7 +182,7 @@ class ClockSampler:
             import pynvml as N
 
             N.nvmlInit()
-            h = N.nvmlDeviceGetHandleByIndex(self.device)
+            h = nvml_handle(N, self.device)
             self.max_mhz = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
             while not self.stop.is_set():
                 mhz = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
@@ -221,6 +221,41 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # replicas: every rank verifies its own batch, no data-path collective
 # ---------------------------------------------------------------------------
+
+def nvml_handle(N, device: int):
+    """The NVML handle of CUDA device `device`, found by PCI bus id (NVML
+    numbers every GPU of the node; CUDA only the visible ones)."""
+    import torch
+
+    pr = torch.cuda.get_device_properties(device)
+    try:
+        return N.nvmlDeviceGetHandleByPciBusId(f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0")
+    except Exception:
+        return N.nvmlDeviceGetHandleByIndex(device)
+
+
+def bind_near_gpu(device: int):
+    """Runs this process on the CPUs NVML reports as nearest the GPU, so the
+    pinned host buffers it allocates afterwards sit on the GPU's NUMA node
+    (host<->device copies from the far node lose bandwidth).  Returns the
+    previous CPU set (None when nothing changed)."""
+    try:
+        import pynvml as N
+
+        N.nvmlInit()
+        n = os.cpu_count() or 1
+        words = N.nvmlDeviceGetCpuAffinity(nvml_handle(N, device), (n + 63) // 64)
+        N.nvmlShutdown()
+        near = {64 * w + b for w, m in enumerate(words) for b in range(64) if (m >> b) & 1}
+        old = os.sched_getaffinity(0)
+        near &= old
+        if near and near != old:
+            os.sched_setaffinity(0, near)
+            return old
+    except Exception:
+        pass
+    return None
+
 
 def verify_launches(xb, count: int, wots_len: int = 67, layers: int = 1, func: int = 0, n: int = 32) -> int:
     """Kernels of one device verify call (csrc/engine.cu Engine::verify): the
@@ -268,6 +303,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
+    cpus_before = bind_near_gpu(local_rank)  # before any pinned allocation
     xb.init(local_rank)
     w = make_workload(xb, rank)
     p = w["p"]
@@ -476,6 +512,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     # ---- CPU baseline (rank 0, N = 1) ----
     cpu = None
+    e2e_cpus = len(os.sched_getaffinity(0))
+    if cpus_before:
+        os.sched_setaffinity(0, cpus_before)  # the CPU baseline uses every host core
     if rank == 0 and world == 1 and not args.skip_cpu:
         cpu = cpu_baseline(w, budget_s=args.cpu_seconds)
 
@@ -508,7 +547,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "e2e": {"value": e2e_value, "unit": "verifies/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "blocking_call_verifies_per_s": NUM_SIGS / blocking_s,
                 "api": "xmss_b200_sign_open_batch_async on two streams (pinned host buffers; copies of every "
-                       "step inside the timed region, L2 flushed before each step)"},
+                       "step inside the timed region, L2 flushed before each step)",
+                "host_cpus": (f"{e2e_cpus} CPUs nearest the GPU "
+                              "(NVML affinity), pinned buffers allocated there") if cpus_before else "all host CPUs"},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "alu", "kernel": "k_verify_chains<Sha256N32>", "achieved": achieved,
                      "peak": probe_rate / 1e9, "unit": "Gcompr/s", "frac": achieved / (probe_rate / 1e9),
