@@ -506,7 +506,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         sec["batch"] = batch_rates(xb, torch, dev, sh)
     if world == 1 and not args.skip_serve:
         sargs = argparse.Namespace(**vars(args))
-        sargs.serve_rates, sargs.serve_n, sargs.serve_seconds = args.sec_serve_rates, 30000, 1.0
+        sargs.serve_rates, sargs.serve_n, sargs.serve_seconds = args.sec_serve_rates, 100000, 1.0
         sargs.serve_plain_n, sargs.serve_check = 60, 1
         sec["serve"] = run_serve(sargs)
 
