@@ -1024,8 +1024,10 @@ def batch_rates(xb, torch, dev, sh, repeats: int = 5):
     """One CUDA graph of keygen, sign and verify groups of three parameter
     sets (two hash families, XMSS and XMSS^MT), timed per launch with CUDA
     events (L2 flushed before each), against the same groups captured one
-    per graph and launched back to back on one stream; outputs checked
-    byte for byte against the per-kind entry points."""
+    per graph and launched back to back on one stream, and as the graph of
+    one persistent launch per hash family (every group's tasks in one device
+    work queue); outputs checked byte for byte against the per-kind entry
+    points."""
     rng = np.random.default_rng(SEED + 5)
     groups, expect, keep = _batch_inputs(xb, torch, dev, rng)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
@@ -1042,17 +1044,20 @@ def batch_rates(xb, torch, dev, sh, repeats: int = 5):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    one, seq = [], []
+    one, seq, pers = [], [], []
     for _ in range(repeats):
         b = xb.Batch(_fresh(groups))
         one.append(timed([b]))
+        b.close()
+        b = xb.Batch(_fresh(groups), persistent=True)
+        pers.append(timed([b]))
         b.close()
         bs = [xb.Batch(_fresh([g])) for g in groups]
         seq.append(timed(bs))
         for x in bs:
             x.close()
-    # outputs of the last sequential launch overwritten by one more batched launch, then checked
-    b = xb.Batch(_fresh(groups))
+    # outputs of the last launches overwritten by one more persistent batch, then checked
+    b = xb.Batch(_fresh(groups), persistent=True)
     assert b.launch(sh) == 0
     torch.cuda.synchronize()
     b.close()
@@ -1098,6 +1103,7 @@ def batch_rates(xb, torch, dev, sh, repeats: int = 5):
     out = {"workload": "mixed batch, one CUDA graph",
            "groups": [{"kind": k, "set": nm, "items": c} for k, nm, _, c, _ in BATCH_GROUPS],
            "items": items, "ms_per_batch": ms, "items_per_s": items / (ms / 1e3),
+           "ms_per_batch_persistent": float(np.median(pers)),
            "ms_groups_one_graph_each_back_to_back": ms_seq, "repeats": repeats,
            "verify_groups_ms": vt,
            "correct": bool(ok), "check": "every key, signature and status equal to the per-kind entry points "

@@ -69,6 +69,7 @@ struct Group {
     uint32_t live = 0;
     std::vector<uint8_t> keys;
     std::vector<uint64_t> idx;
+    std::vector<uint8_t> ib;  // 8 per live item
     DevBuf d_off, d_len, d_ib;
     uint64_t extent = 0;  // bytes of d_sm the live items cover
 
@@ -91,6 +92,8 @@ struct xmss_b200_batch {
     int device = 0;
     bool has_sign = false;
     bool launched = false;
+    bool persistent = false;        // one persistent launch per family instead of the per-group sequences
+    Engine::PersistScratch pscratch;  // its workspaces and counters
     ~xmss_b200_batch()
     {
         if (exec) cudaGraphExecDestroy(exec);
@@ -149,6 +152,7 @@ void prepare(Group& G)
         G.extent = std::max(G.extent, off[r] + p.sig_bytes + len[r]);
     }
     G.live = (uint32_t)G.idx.size();
+    G.ib = ib;
     if (!G.live) return;
     uint64_t* d_off = G.d_off.as<uint64_t>(G.live);
     uint64_t* d_len = G.d_len.as<uint64_t>(G.live);
@@ -186,7 +190,68 @@ void run(Engine& e, Group& G, uint8_t* sm_out)
 
 }  // namespace
 
+namespace {
+
+// The batch's groups as batches of the persistent form; sign groups write
+// into sm_out (the sizing run's scratch) when given.
+std::vector<Engine::PersistJob> persist_jobs(xmss_b200_batch& b, const std::vector<uint8_t*>& sm_out)
+{
+    std::vector<Engine::PersistJob> js;
+    for (size_t i = 0; i < b.groups.size(); i++) {
+        Group& G = *b.groups[i];
+        const xmss_b200_batch_group& g = G.g;
+        Engine::PersistJob j;
+        j.ops = G.ops;
+        j.p = G.p;
+        j.count = g.count;
+        if (g.kind == XMSS_B200_KEYGEN) {
+            j.kind = xb::kJobKeygen;
+            j.d_seeds = g.d_seeds;
+            j.d_pk_out = g.d_pk;
+            j.d_sk_out = g.d_sk;
+        } else if (g.kind == XMSS_B200_VERIFY) {
+            j.kind = xb::kJobVerify;
+            j.d_sm = g.d_sm;
+            j.d_sm_off = g.d_sm_off;
+            j.d_smlen = g.d_len;
+            j.d_pk = g.d_pk;
+            j.npk = g.npk;
+            j.d_pk_index = g.d_pk_index;
+            j.d_status = g.d_status;
+        } else {
+            j.kind = xb::kJobSign;
+            j.count = G.live;
+            if (!G.live) continue;
+            j.h_sk = G.keys.data();
+            j.h_idx = G.idx.data();
+            j.h_ibytes = G.ib.data();
+            j.d_sign_sm = sm_out[i] ? sm_out[i] : g.d_sm;
+            j.d_sm_off = G.d_off.as<uint64_t>(G.live);
+            j.d_mlen = G.d_len.as<uint64_t>(G.live);
+        }
+        js.push_back(j);
+    }
+    return js;
+}
+
+int create(const xmss_b200_batch_group* groups, uint32_t ngroups, xmss_b200_batch** out, bool persistent);
+
+}  // namespace
+
+extern "C" int xmss_b200_batch_create_persistent(const xmss_b200_batch_group* groups, uint32_t ngroups,
+                                                 xmss_b200_batch** out)
+{
+    return create(groups, ngroups, out, true);
+}
+
 extern "C" int xmss_b200_batch_create(const xmss_b200_batch_group* groups, uint32_t ngroups, xmss_b200_batch** out)
+{
+    return create(groups, ngroups, out, false);
+}
+
+namespace {
+
+int create(const xmss_b200_batch_group* groups, uint32_t ngroups, xmss_b200_batch** out, bool persistent)
 {
     if (!groups || !ngroups || !out) {
         xb::set_last_error("xmss_b200_batch_create: bad argument");
@@ -226,8 +291,40 @@ extern "C" int xmss_b200_batch_create(const xmss_b200_batch_group* groups, uint3
             bool prof;
             ~Restore() { e.profiling = prof; }
         } restore{e, prof};
-        // sizing run: every group once, sign groups into wiped scratch
+        b->persistent = persistent;
         XB_CUDA(cudaDeviceSynchronize());  // the caller's buffers are ready
+        if (persistent) {
+            // sizing run of the whole batch (sign groups into wiped scratch),
+            // then the capture of the same launches
+            std::vector<std::unique_ptr<DevBuf>> scratch;
+            std::vector<uint8_t*> sm_out(b->groups.size(), nullptr);
+            for (size_t i = 0; i < b->groups.size(); i++) {
+                Group& G = *b->groups[i];
+                if (G.g.kind != XMSS_B200_SIGN || !G.live) continue;
+                scratch.emplace_back(new DevBuf());
+                sm_out[i] = scratch.back()->as<uint8_t>(G.extent);
+                XB_CUDA(cudaMemcpyAsync(sm_out[i], G.g.d_sm, G.extent, cudaMemcpyDeviceToDevice, b->capture));
+            }
+            e.persistent_multi(persist_jobs(*b, sm_out), b->capture, b->pscratch);
+            for (size_t i = 0; i < b->groups.size(); i++)
+                if (sm_out[i]) XB_CUDA(cudaMemsetAsync(sm_out[i], 0, b->groups[i]->extent, b->capture));
+            XB_CUDA(cudaStreamSynchronize(b->capture));
+            XB_CUDA(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal));
+            try {
+                e.persistent_multi(persist_jobs(*b, std::vector<uint8_t*>(b->groups.size(), nullptr)), b->capture,
+                                   b->pscratch);
+            } catch (...) {
+                cudaGraph_t broken = nullptr;
+                cudaStreamEndCapture(b->capture, &broken);
+                if (broken) cudaGraphDestroy(broken);
+                throw;
+            }
+            XB_CUDA(cudaStreamEndCapture(b->capture, &b->graph));
+            XB_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+            *out = b.release();
+            return 0;
+        }
+        // sizing run: every group once, sign groups into wiped scratch
         for (auto& G : b->groups) {
             DevBuf scratch;
             uint8_t* sm = nullptr;
@@ -267,6 +364,8 @@ extern "C" int xmss_b200_batch_create(const xmss_b200_batch_group* groups, uint3
         return -3;
     }
 }
+
+}  // namespace
 
 extern "C" int xmss_b200_batch_launch(xmss_b200_batch* b, void* stream)
 {

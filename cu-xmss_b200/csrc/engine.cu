@@ -467,6 +467,79 @@ void Engine::verify(const FamilyOps* ops, const xmss_params& p, uint32_t count, 
     XB_CUDA(cudaStreamWaitEvent(st, ss->join, 0));
 }
 
+namespace {
+
+// Keys and subtrees of `count` sign requests, staged to the device.
+struct SignPlan {
+    const uint8_t* keys;      // nkeys rows of SK_SEED | SK_PRF | root | PUB_SEED (4n)
+    const TreeJob* jobs;      // njobs distinct (key, layer, tree) subtrees
+    const uint64_t* tree_off; // [count][d] node array of each request's subtree per layer
+    const uint64_t* idx;      // [count]
+    const uint32_t* key;      // [count] row in keys
+    const uint8_t* ibytes;    // [count][8] index bytes (when given)
+    uint32_t nkeys, njobs;
+};
+
+SignPlan plan_sign(const xmss_params& p, uint32_t count, const uint8_t* h_sk, const uint64_t* h_idx,
+                   const uint8_t* h_ibytes, Workspace& w, cudaStream_t st)
+{
+    const uint32_t n = p.n, th = p.tree_height, d = p.d, ib = p.index_bytes;
+    const uint64_t skb = p.sk_bytes;
+    // Keys: distinct (SK_SEED, SK_PRF, root, PUB_SEED) tuples.
+    std::map<std::string, uint32_t> keyidx;
+    std::vector<uint32_t> req_key(count);
+    std::vector<uint8_t> keymat;  // nkeys x 4n
+    for (uint32_t r = 0; r < count; r++) {
+        std::string k((const char*)h_sk + r * skb + ib, 4 * n);
+        auto it = keyidx.find(k);
+        if (it == keyidx.end()) {
+            it = keyidx.emplace(k, (uint32_t)keyidx.size()).first;
+            keymat.insert(keymat.end(), k.begin(), k.end());
+        }
+        req_key[r] = it->second;
+    }
+    const uint32_t nkeys = (uint32_t)keyidx.size();
+    // Subtrees: distinct (key, layer, tree).
+    const uint64_t tree_bytes = ((2ull << th) - 1) * n;
+    std::map<std::tuple<uint32_t, uint32_t, uint64_t>, uint32_t> jobidx;
+    std::vector<TreeJob> jobs;
+    std::vector<uint64_t> tree_off((size_t)count * d);
+    for (uint32_t r = 0; r < count; r++) {
+        for (uint32_t l = 0; l < d; l++) {
+            const uint32_t sh = th * (l + 1);
+            const uint64_t tree = sh >= 64 ? 0 : (h_idx[r] >> sh);
+            auto key = std::make_tuple(req_key[r], l, tree);
+            auto it = jobidx.find(key);
+            if (it == jobidx.end()) {
+                it = jobidx.emplace(key, (uint32_t)jobs.size()).first;
+                jobs.push_back(TreeJob{req_key[r], l, tree, (uint64_t)jobs.size() * tree_bytes});
+            }
+            tree_off[(size_t)r * d + l] = jobs[it->second].node_off;
+        }
+    }
+    const uint32_t njobs = (uint32_t)jobs.size();
+    // Stage everything in one pinned block and one device block.
+    const size_t sz_keys = (size_t)nkeys * 4 * n, sz_jobs = njobs * sizeof(TreeJob),
+                 sz_toff = tree_off.size() * sizeof(uint64_t), sz_idx = count * sizeof(uint64_t),
+                 sz_key = count * sizeof(uint32_t), sz_ib = h_ibytes ? (size_t)count * 8 : 0;
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t o_jobs = al(sz_keys), o_toff = o_jobs + al(sz_jobs), o_idx = o_toff + al(sz_toff),
+                 o_key = o_idx + al(sz_idx), o_ib = o_key + al(sz_key), total = o_ib + al(sz_ib);
+    uint8_t* hs = w.h_jobs.as<uint8_t>(total);
+    memcpy(hs, keymat.data(), sz_keys);
+    memcpy(hs + o_jobs, jobs.data(), sz_jobs);
+    memcpy(hs + o_toff, tree_off.data(), sz_toff);
+    memcpy(hs + o_idx, h_idx, sz_idx);
+    memcpy(hs + o_key, req_key.data(), sz_key);
+    if (sz_ib) memcpy(hs + o_ib, h_ibytes, sz_ib);
+    uint8_t* ds = w.keys.as<uint8_t>(total);
+    XB_CUDA(cudaMemcpyAsync(ds, hs, total, cudaMemcpyHostToDevice, st));
+    return SignPlan{ds, (const TreeJob*)(ds + o_jobs), (const uint64_t*)(ds + o_toff), (const uint64_t*)(ds + o_idx),
+                    (const uint32_t*)(ds + o_key), sz_ib ? ds + o_ib : nullptr, nkeys, njobs};
+}
+
+}  // namespace
+
 void Engine::persist_setup(const PersistJob& j, Workspace& w, VerifyArgs& v, PersistArgs& q, cudaStream_t st)
 {
     const FamilyOps* ops = j.ops;
@@ -526,13 +599,102 @@ void Engine::verify_persistent(const FamilyOps* ops, const xmss_params& p, uint3
     if (!count) return;
     VerifyArgs v;
     PersistArgs q;
-    persist_setup(PersistJob{ops, p, count, d_sm, d_sm_off, d_smlen, d_pk, npk, d_pk_index, d_status}, ws_, v, q,
-                  st);
+    PersistJob j;
+    j.ops = ops;
+    j.p = p;
+    j.count = count;
+    j.d_sm = d_sm;
+    j.d_sm_off = d_sm_off;
+    j.d_smlen = d_smlen;
+    j.d_pk = d_pk;
+    j.npk = npk;
+    j.d_pk_index = d_pk_index;
+    j.d_status = d_status;
+    persist_setup(j, ws_, v, q, st);
     ops->verify_persist(v, q, st);
     XB_CUDA(cudaGetLastError());
 }
 
-void Engine::verify_persistent_multi(const std::vector<PersistJob>& jobs, cudaStream_t st)
+void Engine::gen_setup(const PersistJob& j, Workspace& w, PersistBatch& J, cudaStream_t st)
+{
+    const FamilyOps* ops = j.ops;
+    const xmss_params& p = j.p;
+    const uint32_t n = p.n, len = ops->len, h = p.tree_height;
+    J = PersistBatch{};
+    J.kind = j.kind;
+    TreeTask& T = J.t;
+    if (j.kind == kJobKeygen) {
+        // one top-layer subtree per key (xmss_core.c:134-161)
+        const uint64_t tree_bytes = ((2ull << h) - 1) * n;
+        TreeJob* hj = w.h_jobs.as<TreeJob>(j.count);
+        for (uint32_t k = 0; k < j.count; k++) hj[k] = TreeJob{k, p.d - 1, 0, (uint64_t)k * tree_bytes};
+        TreeJob* dj = w.jobs.as<TreeJob>(j.count);
+        XB_CUDA(cudaMemcpyAsync(dj, hj, j.count * sizeof(TreeJob), cudaMemcpyHostToDevice, st));
+        T.trees = dj;
+        T.ntrees = T.nkeys = j.count;
+        T.keys = j.d_seeds;  // SK_SEED || SK_PRF || PUB_SEED
+        T.key_stride = 3 * n;
+        T.off_pub = 2 * n;
+        T.off_sks = 0;
+        T.off_skp = n;
+        T.seeds = j.d_seeds;
+        T.pk = j.d_pk_out;
+        T.sk = j.d_sk_out;
+        T.index_bytes = p.index_bytes;
+        T.sk_bytes = (uint32_t)p.sk_bytes;
+    } else {
+        const SignPlan sp = plan_sign(p, j.count, j.h_sk, j.h_idx, j.h_ibytes, w, st);
+        T.trees = sp.jobs;
+        T.ntrees = sp.njobs;
+        T.nkeys = sp.nkeys;
+        T.keys = sp.keys;  // SK_SEED | SK_PRF | root | PUB_SEED
+        T.key_stride = 4 * n;
+        T.off_pub = 3 * n;
+        T.off_sks = 0;
+        T.off_skp = n;
+        T.ibytes = sp.ibytes;
+        SignArgs& g = J.g;
+        g.sm = j.d_sign_sm;
+        g.sm_off = j.d_sm_off;
+        g.mlen = j.d_mlen;
+        g.msg = nullptr;
+        g.msg_off = nullptr;
+        g.idx = sp.idx;
+        g.key = sp.key;
+        g.key_root = sp.keys + 2 * n;
+        g.key_stride = 4 * n;
+        g.tree_off = sp.tree_off;
+        g.lens = w.lens.as<uint8_t>((size_t)j.count * p.d * len);
+        g.count = j.count;
+        g.index_bytes = p.index_bytes;
+        g.sig_bytes = p.sig_bytes;
+        g.tree_height = h;
+        g.d = p.d;
+    }
+    T.h = h;
+    const uint64_t tree_bytes = ((2ull << h) - 1) * n;
+    T.nodes = w.nodes.as<uint8_t>(T.ntrees * tree_bytes);
+    J.g.nodes = T.nodes;
+    const uint64_t slots = (uint64_t)T.ntrees << h;
+    T.wpk = w.wpk.as<uint8_t>(slots * len * n);
+    T.wpk2 = w.wpk2.as<uint8_t>(slots * ((len + 1) / 2) * n);
+    // state: header, per leaf group the chain and L-tree counters, per
+    // subtree its level counters, subtrees done, preparation tasks done
+    const size_t groups = slots >> 5;
+    const size_t words = 4 + groups * 9 + (size_t)T.ntrees * (h + 1) + 2;
+    uint32_t* u = w.pstate.as<uint32_t>(words);
+    J.q.hdr = u;
+    T.chains_done = u + 4;
+    T.lt_done = T.chains_done + groups;
+    T.lvl_done = T.lt_done + 8 * groups;
+    T.trees_done = T.lvl_done + (size_t)T.ntrees * (h + 1);
+    T.prep_done = T.trees_done + 1;
+    J.q.ctx = w.ctx.get((size_t)T.nkeys * ops->ctx_bytes);
+    J.q.wait_ns = persist_wait_ns;
+    XB_CUDA(cudaMemsetAsync(u, 0, words * 4, st));
+}
+
+void Engine::persistent_multi(const std::vector<PersistJob>& jobs, cudaStream_t st, PersistScratch& scratch)
 {
     XB_CUDA(cudaMemsetAsync(work_, 0, 3 * sizeof(unsigned long long), st));
     // launches: the batches of one family, at most kMaxPersistJobs each
@@ -548,7 +710,7 @@ void Engine::verify_persistent_multi(const std::vector<PersistJob>& jobs, cudaSt
         launches[open[jobs[i].ops]].push_back(i);
     }
     if (launches.empty()) return;
-    while (pws_.size() < jobs.size()) pws_.emplace_back(new Workspace());
+    while (scratch.ws.size() < jobs.size()) scratch.ws.emplace_back(new Workspace());
     while (pstreams_.size() + 1 < launches.size()) {
         cudaStream_t s;
         cudaEvent_t e;
@@ -559,7 +721,7 @@ void Engine::verify_persistent_multi(const std::vector<PersistJob>& jobs, cudaSt
     }
     if (!pfork_) XB_CUDA(cudaEventCreateWithFlags(&pfork_, cudaEventDisableTiming));
     // a ticket counter and an exit counter per launch, zeroed before the fork
-    unsigned long long* ctr = pctr_.as<unsigned long long>(2 * launches.size());
+    unsigned long long* ctr = scratch.ctr.as<unsigned long long>(2 * launches.size());
     XB_CUDA(cudaMemsetAsync(ctr, 0, 2 * launches.size() * sizeof(unsigned long long), st));
     XB_CUDA(cudaEventRecord(pfork_, st));
     for (size_t l = 0; l < launches.size(); l++) {
@@ -569,31 +731,45 @@ void Engine::verify_persistent_multi(const std::vector<PersistJob>& jobs, cudaSt
         P.njobs = (uint32_t)launches[l].size();
         P.ticket = ctr + 2 * l;
         P.exited = (uint32_t*)(ctr + 2 * l + 1);
-        uint32_t phases = 0;
+        uint32_t phases = 1;
         for (uint32_t k = 0; k < P.njobs; k++) {
             const size_t i = launches[l][k];
-            persist_setup(jobs[i], *pws_[i], P.v[k], P.q[k], s);
-            phases = std::max(phases, 1 + P.v[k].d);
+            PersistBatch& J = P.job[k];
+            if (jobs[i].kind == kJobVerify) {
+                J = PersistBatch{};
+                J.kind = kJobVerify;
+                persist_setup(jobs[i], *scratch.ws[i], J.v, J.q, s);
+                phases = std::max(phases, 1 + J.v.d);
+            } else {
+                gen_setup(jobs[i], *scratch.ws[i], J, s);
+            }
         }
-        // segments: phase 0 (contexts, H_msg, h_pre) of every batch, then
-        // each layer of every batch that has it
+        // segments: phase 0 of every batch (a verify batch's contexts, H_msg
+        // and h_pre; a whole keygen or sign batch), then each layer of every
+        // verify batch that has it
         P.nsegs = 0;
         P.first[0] = 0;
         for (uint32_t ph = 0; ph < phases; ph++) {
             for (uint32_t k = 0; k < P.njobs; k++) {
-                const VerifyArgs& v = P.v[k];
-                const PersistArgs& q = P.q[k];
-                if (ph > v.d) continue;
+                const PersistBatch& J = P.job[k];
                 const unsigned long long len = jobs[launches[l][k]].ops->len;
-                const unsigned long long G = q.groups, K = (q.npk + 31) / 32;
-                const unsigned long long head = K + G + G * v.d * (len - 1 + v.tree_height);
-                const unsigned long long per_layer = persist_total((int)len, q.groups, q.npk, 1, v.tree_height) -
-                                                     (K + G + G * (len - 1 + v.tree_height));
-                const unsigned long long a = ph == 0 ? 0 : head + (ph - 1) * per_layer;
-                const unsigned long long n = ph == 0 ? head : per_layer;
-                P.job[P.nsegs] = (uint8_t)k;
+                unsigned long long a = 0, cnt = 0;
+                if (J.kind != kJobVerify) {
+                    if (ph) continue;
+                    cnt = gen_total(J, (int)len);
+                } else {
+                    const VerifyArgs& v = J.v;
+                    const PersistArgs& q = J.q;
+                    if (ph > v.d) continue;
+                    const unsigned long long G = q.groups, K = (q.npk + 31) / 32;
+                    const unsigned long long head = K + G + G * v.d * (len - 1 + v.tree_height);
+                    const unsigned long long per_layer = G * (len + lt_items_total((int)len) + 1);
+                    a = ph == 0 ? 0 : head + (ph - 1) * per_layer;
+                    cnt = ph == 0 ? head : per_layer;
+                }
+                P.seg_job[P.nsegs] = (uint8_t)k;
                 P.local0[P.nsegs] = a;
-                P.first[P.nsegs + 1] = P.first[P.nsegs] + n;
+                P.first[P.nsegs + 1] = P.first[P.nsegs] + cnt;
                 P.nsegs++;
             }
         }
@@ -613,82 +789,35 @@ void Engine::last_verify_work(unsigned long long out[3])
     XB_CUDA(cudaMemcpy(out, work_, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
 }
 
+
 void Engine::sign(const FamilyOps* ops, const xmss_params& p, uint32_t count, const uint8_t* h_sk,
                   const uint64_t* h_idx, uint8_t* d_sm, const uint64_t* d_sm_off, const uint64_t* d_mlen,
                   cudaStream_t st, Workspace& w, bool wait)
 {
     if (!count) return;
-    const uint32_t n = p.n, th = p.tree_height, d = p.d, ib = p.index_bytes;
-    const uint64_t skb = p.sk_bytes;
-    // Keys: distinct (SK_SEED, SK_PRF, root, PUB_SEED) tuples.
-    std::map<std::string, uint32_t> keyidx;
-    std::vector<uint32_t> req_key(count);
-    std::vector<uint8_t> keymat;  // nkeys x 4n
-    for (uint32_t r = 0; r < count; r++) {
-        std::string k((const char*)h_sk + r * skb + ib, 4 * n);
-        auto it = keyidx.find(k);
-        if (it == keyidx.end()) {
-            it = keyidx.emplace(k, (uint32_t)keyidx.size()).first;
-            keymat.insert(keymat.end(), k.begin(), k.end());
-        }
-        req_key[r] = it->second;
-    }
-    const uint32_t nkeys = (uint32_t)keyidx.size();
-    // Subtrees: distinct (key, layer, tree).
-    const uint64_t tree_bytes = ((2ull << th) - 1) * n;
-    std::map<std::tuple<uint32_t, uint32_t, uint64_t>, uint32_t> jobidx;
-    std::vector<TreeJob> jobs;
-    std::vector<uint64_t> tree_off((size_t)count * d);
-    for (uint32_t r = 0; r < count; r++) {
-        for (uint32_t l = 0; l < d; l++) {
-            const uint32_t sh = th * (l + 1);
-            const uint64_t tree = sh >= 64 ? 0 : (h_idx[r] >> sh);
-            auto key = std::make_tuple(req_key[r], l, tree);
-            auto it = jobidx.find(key);
-            if (it == jobidx.end()) {
-                it = jobidx.emplace(key, (uint32_t)jobs.size()).first;
-                jobs.push_back(TreeJob{req_key[r], l, tree, (uint64_t)jobs.size() * tree_bytes});
-            }
-            tree_off[(size_t)r * d + l] = jobs[it->second].node_off;
-        }
-    }
-    const uint32_t njobs = (uint32_t)jobs.size();
-    // Stage everything in one pinned block and one device block.
-    const size_t sz_keys = (size_t)nkeys * 4 * n, sz_jobs = njobs * sizeof(TreeJob),
-                 sz_toff = tree_off.size() * sizeof(uint64_t), sz_idx = count * sizeof(uint64_t),
-                 sz_key = count * sizeof(uint32_t);
-    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t o_jobs = al(sz_keys), o_toff = o_jobs + al(sz_jobs), o_idx = o_toff + al(sz_toff),
-                 o_key = o_idx + al(sz_idx), total = o_key + al(sz_key);
-    uint8_t* hs = w.h_jobs.as<uint8_t>(total);
-    memcpy(hs, keymat.data(), sz_keys);
-    memcpy(hs + o_jobs, jobs.data(), sz_jobs);
-    memcpy(hs + o_toff, tree_off.data(), sz_toff);
-    memcpy(hs + o_idx, h_idx, sz_idx);
-    memcpy(hs + o_key, req_key.data(), sz_key);
-    uint8_t* ds = w.keys.as<uint8_t>(total);
-    XB_CUDA(cudaMemcpyAsync(ds, hs, total, cudaMemcpyHostToDevice, st));
-    const uint8_t* dkeys = ds;
-    void* ctx = w.ctx.get((size_t)nkeys * ops->ctx_bytes);
+    const uint32_t n = p.n, th = p.tree_height, d = p.d;
+    const SignPlan sp = plan_sign(p, count, h_sk, h_idx, nullptr, w, st);
+    void* ctx = w.ctx.get((size_t)sp.nkeys * ops->ctx_bytes);
     // key material rows: SK_SEED | SK_PRF | root | PUB_SEED
-    ops->make_ctx(dkeys + 3 * n, 4 * n, dkeys, 4 * n, dkeys + n, 4 * n, nkeys, ctx, st);
-    uint8_t* nodes = w.nodes.as<uint8_t>(njobs * tree_bytes);
-    build_trees(ops, (const TreeJob*)(ds + o_jobs), njobs, (int)th, nodes, ctx, st, w, subtree_k(p, njobs));
+    ops->make_ctx(sp.keys + 3 * n, 4 * n, sp.keys, 4 * n, sp.keys + n, 4 * n, sp.nkeys, ctx, st);
+    const uint64_t tree_bytes = ((2ull << th) - 1) * n;
+    uint8_t* nodes = w.nodes.as<uint8_t>(sp.njobs * tree_bytes);
+    build_trees(ops, sp.jobs, sp.njobs, (int)th, nodes, ctx, st, w, subtree_k(p, sp.njobs));
     SignArgs g;
     g.sm = d_sm;
     g.sm_off = d_sm_off;
     g.mlen = d_mlen;
     g.msg = nullptr;  // messages follow the signatures in d_sm
     g.msg_off = nullptr;
-    g.idx = (const uint64_t*)(ds + o_idx);
-    g.key = (const uint32_t*)(ds + o_key);
-    g.key_root = dkeys + 2 * n;
+    g.idx = sp.idx;
+    g.key = sp.key;
+    g.key_root = sp.keys + 2 * n;
     g.key_stride = 4 * n;
-    g.tree_off = (const uint64_t*)(ds + o_toff);
+    g.tree_off = sp.tree_off;
     g.nodes = nodes;
     g.lens = w.lens.as<uint8_t>((size_t)count * d * ops->len);
     g.count = count;
-    g.index_bytes = ib;
+    g.index_bytes = p.index_bytes;
     g.sig_bytes = p.sig_bytes;
     g.tree_height = th;
     g.d = d;

@@ -21,6 +21,7 @@ namespace xb {
 struct LeafRef;
 struct TreeJob;
 struct VerifyArgs;
+struct PersistBatch;
 
 class CudaFailure : public std::runtime_error {
    public:
@@ -171,22 +172,48 @@ class Engine {
                            const uint32_t* d_pk_index, int* d_status, cudaStream_t st);
 
     // One verify batch of the persistent form (device pointers).
+    // A keygen or sign batch of the persistent form.
     struct PersistJob {
-        const FamilyOps* ops;
-        xmss_params p;
-        uint32_t count;
-        const uint8_t* d_sm;
-        const uint64_t* d_sm_off;
-        const uint64_t* d_smlen;
-        const uint8_t* d_pk;
-        uint32_t npk;
-        const uint32_t* d_pk_index;
-        int* d_status;
+        uint32_t kind = 0;  // 0 verify, 1 keygen, 2 sign
+        const FamilyOps* ops = nullptr;
+        xmss_params p{};
+        uint32_t count = 0;
+        // verify
+        const uint8_t* d_sm = nullptr;
+        const uint64_t* d_sm_off = nullptr;
+        const uint64_t* d_smlen = nullptr;
+        const uint8_t* d_pk = nullptr;
+        uint32_t npk = 0;
+        const uint32_t* d_pk_index = nullptr;
+        int* d_status = nullptr;
+        // keygen: seeds (count x 3n) -> pk (count x 2n), sk (count x sk_bytes)
+        const uint8_t* d_seeds = nullptr;
+        uint8_t* d_pk_out = nullptr;
+        uint8_t* d_sk_out = nullptr;
+        // sign: per item the key as it signs (sk without OID, after the index
+        // bookkeeping), the index and the index bytes of the signature (8 per
+        // item), host memory read at setup; d_sm / d_sm_off / d_mlen as Engine::sign
+        const uint8_t* h_sk = nullptr;
+        const uint64_t* h_idx = nullptr;
+        const uint8_t* h_ibytes = nullptr;
+        uint8_t* d_sign_sm = nullptr;
+        const uint64_t* d_mlen = nullptr;
     };
-    // Batches of any parameter sets: one persistent launch per hash family
-    // (up to 8 batches each), the families' launches on streams forked from
-    // st and joined back into it.
-    void verify_persistent_multi(const std::vector<PersistJob>& jobs, cudaStream_t st);
+    // Scratch of persistent multi-batch launches: a workspace per batch and
+    // the launches' ticket / exit counters (the engine keeps one for its own
+    // calls; a captured graph keeps its own).
+    struct PersistScratch {
+        std::vector<std::unique_ptr<Workspace>> ws;
+        DevBuf ctr;
+    };
+    // Batches of any parameter sets and kinds: one persistent launch per hash
+    // family (up to 8 batches each), the families' launches on streams forked
+    // from st and joined back into it.
+    void verify_persistent_multi(const std::vector<PersistJob>& jobs, cudaStream_t st)
+    {
+        persistent_multi(jobs, st, pscratch_);
+    }
+    void persistent_multi(const std::vector<PersistJob>& jobs, cudaStream_t st, PersistScratch& scratch);
 
     // Key generation from seeds (count x 3n) into pk (count x 2n) and sk
     // (count x sk_bytes), no OID prefix.
@@ -264,8 +291,9 @@ class Engine {
     // persistent batches: arguments of one batch over workspace w, its task
     // counters zeroed on st
     void persist_setup(const PersistJob& j, Workspace& w, VerifyArgs& v, PersistArgs& q, cudaStream_t st);
-    std::vector<std::unique_ptr<Workspace>> pws_;  // one per batch of a multi-batch launch
-    DevBuf pctr_;                                  // ticket and exit counters of those launches
+    // a keygen or sign batch of a multi-batch launch
+    void gen_setup(const PersistJob& j, Workspace& w, PersistBatch& J, cudaStream_t st);
+    PersistScratch pscratch_;
     std::vector<cudaStream_t> pstreams_;           // launches after the first
     std::vector<cudaEvent_t> pjoin_;
     cudaEvent_t pfork_ = nullptr;

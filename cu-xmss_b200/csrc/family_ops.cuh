@@ -190,17 +190,27 @@ struct Launch {
         }();
         k_verify_persist<F, FT><<<grid, 128, 0, st>>>(v, q);
     }
-    static void verify_persist_multi(const PersistJobs& P, cudaStream_t st)
+    template <bool GEN>
+    static unsigned persist_multi_grid()
     {
-        if (!P.njobs) return;
         static const unsigned grid = [] {
             int dev = 0, sms = 0, per = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_verify_persist_multi<F, FT>, 128, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_verify_persist_multi<F, FT, GEN>, 128, 0);
             return (unsigned)(sms * (per > 0 ? per : 1));
         }();
-        k_verify_persist_multi<F, FT><<<grid, 128, 0, st>>>(P);
+        return grid;
+    }
+    static void verify_persist_multi(const PersistJobs& P, cudaStream_t st)
+    {
+        if (!P.njobs) return;
+        bool gen = false;
+        for (uint32_t k = 0; k < P.njobs; k++) gen |= P.job[k].kind != kJobVerify;
+        if (gen)
+            k_verify_persist_multi<F, FT, true><<<persist_multi_grid<true>(), 128, 0, st>>>(P);
+        else
+            k_verify_persist_multi<F, FT, false><<<persist_multi_grid<false>(), 128, 0, st>>>(P);
     }
     static void sign_prep(const SignArgs& g, const void* ctx, cudaStream_t st)
     {

@@ -16,6 +16,9 @@ struct SignArgs;
 struct PersistArgs;
 struct PersistJobs;
 
+// Kinds of the batches of a persistent multi-batch launch.
+enum : uint32_t { kJobVerify = 0, kJobKeygen = 1, kJobSign = 2 };
+
 struct FamilyOps {
     const char* name;
     unsigned func, n, len;

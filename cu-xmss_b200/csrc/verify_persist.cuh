@@ -33,6 +33,7 @@
 // only the schedule differs).
 #pragma once
 
+#include "family_ops.h"
 #include "xmss_kernels.cuh"
 
 namespace xb {
@@ -458,32 +459,262 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>()) k_verify_persist(c
     }
 }
 
+// Keygen and sign batches inside a persistent launch.  Their subtrees (all
+// of height h) are built by tasks of the same queue:
+//   ctx     32 keys: PUB_SEED / SK_SEED / SK_PRF midstates            (no deps)
+//   chain   chain c of 32 leaves (a lane each): PRF_keygen + 15 F     (ctx)
+//   ltree   one pair index of one L-tree level of those 32 leaves     (chains / level below)
+//   merkle  32 nodes of one level of one subtree                      (leaf groups / level below)
+// then, for keygen, one task per key writing pk and sk (its tree), and for
+// sign, the preparation of 32 signatures (R, H_msg, chain lengths, auth
+// paths; every subtree built) and the signature chains, 32 at a time (their
+// preparation).  Ticket order: ctx, chains (leaf-group major), L-tree levels,
+// Merkle levels (level major), then the tail; each task waits only on
+// smaller tickets.  Leaf groups never straddle subtrees: h >= 5 in every
+// parameter set.
+
+struct TreeTask {
+    const TreeJob* trees;   // [ntrees]: key, layer, tree, node_off
+    uint32_t ntrees, h;
+    uint8_t* nodes;         // node arrays
+    uint8_t* wpk;           // [ntrees << h][LEN][n] WOTS public keys
+    uint8_t* wpk2;          // [ntrees << h][(LEN + 1) / 2][n] (L-tree ping-pong)
+    const uint8_t* keys;    // key material rows the contexts are made from
+    uint32_t key_stride, off_pub, off_sks, off_skp, nkeys;
+    uint32_t* chains_done;  // [leaf groups] chain tasks finished
+    uint32_t* lt_done;      // [leaf groups][8] L-tree level tasks finished
+    uint32_t* lvl_done;     // [ntrees][h + 1] level 0: leaf groups done; level m: its Merkle tasks
+    uint32_t* trees_done;   // subtrees complete
+    uint32_t* prep_done;    // sign preparation tasks finished
+    const uint8_t* seeds;   // keygen: [ntrees][3n] SK_SEED || SK_PRF || PUB_SEED
+    uint8_t* pk;            // keygen: [ntrees][2n]
+    uint8_t* sk;            // keygen: [ntrees][sk_bytes]
+    uint32_t index_bytes, sk_bytes;
+    const uint8_t* ibytes;  // sign: [count][8] the index bytes of each signature
+};
+
+struct PersistBatch {
+    uint32_t kind;   // kJobVerify, kJobKeygen, kJobSign
+    VerifyArgs v;    // verify
+    PersistArgs q;   // hdr (error flag, CTAs out, contexts done), ctx, wait_ns: every kind
+    TreeTask t;      // keygen, sign
+    SignArgs g;      // sign
+};
+
+// Merkle tasks of level m (nodes of level m + 1 in groups of 32) per subtree.
+__host__ __device__ inline unsigned long long merkle_chunks(uint32_t h, uint32_t m)
+{
+    return ((1ull << (h - m - 1)) + 31) / 32;
+}
+
+// Ticket counts of a keygen or sign batch: [0] ctx, [1] chains, [2] L-tree,
+// [3] Merkle, [4] tail (keygen: one per key; sign: preparation), [5] sign
+// chains.
+__host__ __device__ inline void gen_counts(const PersistBatch& J, int len, unsigned long long (&c)[6])
+{
+    const TreeTask& t = J.t;
+    const unsigned long long groups = ((unsigned long long)t.ntrees << t.h) >> 5;
+    c[0] = (t.nkeys + 31) / 32;
+    c[1] = groups * len;
+    c[2] = groups * lt_items_total(len);
+    c[3] = 0;
+    for (uint32_t m = 0; m < t.h; m++) c[3] += t.ntrees * merkle_chunks(t.h, m);
+    if (J.kind == kJobKeygen) {
+        c[4] = t.ntrees;
+        c[5] = 0;
+    } else {
+        c[4] = (J.g.count + 31) / 32;
+        c[5] = ((unsigned long long)J.g.count * J.g.d * len + 31) / 32;
+    }
+}
+
+__host__ __device__ inline unsigned long long gen_total(const PersistBatch& J, int len)
+{
+    unsigned long long c[6];
+    gen_counts(J, len, c);
+    return c[0] + c[1] + c[2] + c[3] + c[4] + c[5];
+}
+
+// Runs ticket t of a keygen or sign batch (whole warp); false when a wait
+// ran out or the batch failed.
+template <class F, class FT>
+__device__ __forceinline__ bool gen_step(const PersistBatch& J, unsigned long long t)
+{
+    using Ctx = typename F::Ctx;
+    constexpr int LEN = F::LEN, N = F::N;
+    const TreeTask& T = J.t;
+    const PersistArgs& q = J.q;
+    const uint32_t lane = threadIdx.x & 31, h = T.h;
+    uint32_t* err = q.hdr;
+    Ctx* ctx = (Ctx*)q.ctx;
+    unsigned long long c[6];
+    gen_counts(J, LEN, c);
+    if (t < c[0]) {  // -------- contexts of 32 keys
+        const uint32_t k = (uint32_t)t * 32 + lane;
+        if (k < T.nkeys) {
+            const uint8_t* row = T.keys + (uint64_t)k * T.key_stride;
+            Ctx x;
+            F::make_ctx(x, row + T.off_pub, row + T.off_sks, row + T.off_skp);
+            ctx[k] = x;
+        }
+        persist_signal(&q.hdr[2]);
+        return true;
+    }
+    t -= c[0];
+    if (t < c[1]) {  // -------- chain c of 32 leaves: wots_pkgen's chain (PRF_keygen + 15 F)
+        const uint32_t grp = (uint32_t)(t / LEN), ch = (uint32_t)(t - (unsigned long long)grp * LEN);
+        if (!persist_wait(&q.hdr[2], (uint32_t)c[0], err, q.wait_ns)) return false;
+        const uint64_t slot = (uint64_t)grp * 32 + lane;
+        const TreeJob tj = T.trees[slot >> h];
+        const uint32_t leaf = (uint32_t)(slot & ((1ull << h) - 1));
+        const typename FT::Ctx kc = ((const typename FT::Ctx*)ctx)[tj.key];
+        uint32_t a[8], x[F::NW];
+        set_addr(a, tj.layer, tj.tree, ADDR_OTS, leaf, ch, 0);
+        run_chain<FT>(x, kc, a, 0, 15, true);
+        F::store(T.wpk + (slot * LEN + ch) * N, x);
+        persist_signal(&T.chains_done[grp]);
+        return true;
+    }
+    t -= c[1];
+    if (t < c[2]) {  // -------- one pair index of one L-tree level of 32 leaves
+        const unsigned long long groups = c[1] / LEN;
+        int lev = 0;
+        while (t >= groups * lt_items(LEN, lev)) {
+            t -= groups * lt_items(LEN, lev);
+            lev++;
+        }
+        const uint32_t items = (uint32_t)lt_items(LEN, lev);
+        const uint32_t grp = (uint32_t)(t / items), p = (uint32_t)(t - (unsigned long long)grp * items);
+        if (lev == 0) {
+            if (!persist_wait(&T.chains_done[grp], (uint32_t)LEN, err, q.wait_ns)) return false;
+        } else if (!persist_wait(&T.lt_done[grp * 8 + lev - 1], (uint32_t)lt_items(LEN, lev - 1), err, q.wait_ns)) {
+            return false;
+        }
+        const uint64_t slot = (uint64_t)grp * 32 + lane;
+        const uint32_t j = (uint32_t)(slot >> h);
+        const TreeJob tj = T.trees[j];
+        const uint32_t leaf = (uint32_t)(slot & ((1ull << h) - 1));
+        const int cin = lt_cnt(LEN, lev);
+        const bool even = (lev & 1) == 0;
+        const uint8_t* src = even ? T.wpk + slot * LEN * N : T.wpk2 + slot * ((LEN + 1) / 2) * N;
+        uint8_t* out = (cin == 2) ? T.nodes + tj.node_off + (level_offset((int)h, 0) + leaf) * N
+                       : even     ? T.wpk2 + (slot * ((LEN + 1) / 2) + p) * N
+                                  : T.wpk + (slot * LEN + p) * N;
+        uint32_t l[F::NW], o[F::NW];
+        F::load(l, src + (uint64_t)(2 * p) * N);
+        if (2 * (int)p + 1 < cin) {
+            uint32_t rr[F::NW], a[8];
+            F::load(rr, src + (uint64_t)(2 * p + 1) * N);
+            set_addr(a, tj.layer, tj.tree, ADDR_LTREE, leaf, (uint32_t)lev, p);
+            F::thash_h(o, l, rr, ctx[tj.key], a);
+            F::store(out, o);
+        } else {
+            F::store(out, l);
+        }
+        persist_signal(&T.lt_done[grp * 8 + lev]);
+        // the leaf group's last level completes a group of its subtree's leaves
+        if (cin == 2) persist_signal(&T.lvl_done[j * (h + 1)]);
+        return true;
+    }
+    t -= c[2];
+    if (t < c[3]) {  // -------- 32 nodes of Merkle level m + 1 of one subtree
+        uint32_t m = 0;
+        while (t >= T.ntrees * merkle_chunks(h, m)) {
+            t -= T.ntrees * merkle_chunks(h, m);
+            m++;
+        }
+        const unsigned long long per = merkle_chunks(h, m);
+        const uint32_t j = (uint32_t)(t / per), ck = (uint32_t)(t - (unsigned long long)j * per);
+        const uint32_t need = m == 0 ? (1u << h) / 32 : (uint32_t)merkle_chunks(h, m - 1);
+        if (!persist_wait(&T.lvl_done[j * (h + 1) + m], need, err, q.wait_ns)) return false;
+        const TreeJob tj = T.trees[j];
+        uint8_t* base = T.nodes + tj.node_off;
+        const uint32_t i = ck * 32 + lane;
+        if (i < (1u << (h - m - 1))) {
+            uint32_t l[F::NW], r[F::NW], o[F::NW], a[8];
+            F::load(l, base + (level_offset((int)h, (int)m) + 2ull * i) * N);
+            F::load(r, base + (level_offset((int)h, (int)m) + 2ull * i + 1) * N);
+            set_addr(a, tj.layer, tj.tree, ADDR_HASHTREE, 0, m, i);
+            F::thash_h(o, l, r, ctx[tj.key], a);
+            F::store(base + (level_offset((int)h, (int)m + 1) + i) * N, o);
+        }
+        persist_signal(&T.lvl_done[j * (h + 1) + m + 1]);
+        if (m + 1 == h) persist_signal(T.trees_done);
+        return true;
+    }
+    t -= c[3];
+    if (J.kind == kJobKeygen) {  // -------- pk and sk of key t (xmss_core.c:134-161)
+        const uint32_t k = (uint32_t)t;
+        if (!persist_wait(&T.lvl_done[k * (h + 1) + h], 1u, err, q.wait_ns)) return false;
+        const uint8_t* seed = T.seeds + (uint64_t)k * 3 * N;
+        const uint8_t* root = T.nodes + T.trees[k].node_off + level_offset((int)h, (int)h) * N;
+        uint8_t* P = T.pk + (uint64_t)k * 2 * N;
+        uint8_t* S = T.sk + (uint64_t)k * T.sk_bytes;
+        const uint32_t ib = T.index_bytes;
+        for (uint32_t i = lane; i < (uint32_t)N; i += 32) {
+            P[i] = root[i];
+            P[N + i] = seed[2 * N + i];
+            S[ib + i] = seed[i];
+            S[ib + N + i] = seed[N + i];
+            S[ib + 2 * N + i] = root[i];
+            S[ib + 3 * N + i] = seed[2 * N + i];
+        }
+        for (uint32_t i = lane; i < ib; i += 32) S[i] = 0;
+        return true;
+    }
+    const SignArgs& g = J.g;
+    if (t < c[4]) {  // -------- preparation of 32 signatures (every subtree built)
+        if (!persist_wait(T.trees_done, T.ntrees, err, q.wait_ns)) return false;
+        const uint32_t s = (uint32_t)t * 32 + lane;
+        if (s < g.count) {
+            sign_prep_one<F>(g, ctx, s);
+            uint8_t* sm = g.sm + g.sm_off[s];
+            for (uint32_t i = 0; i < g.index_bytes; i++) sm[i] = T.ibytes[(uint64_t)s * 8 + i];
+        }
+        persist_signal(T.prep_done);
+        return true;
+    }
+    t -= c[4];
+    {  // -------- 32 signature chains (wots_sign, wots.c:136-154)
+        if (!persist_wait(T.prep_done, (uint32_t)c[4], err, q.wait_ns)) return false;
+        const uint64_t item = t * 32 + lane;
+        if (item < (uint64_t)g.count * g.d * LEN) {
+            const typename FT::Ctx kc = ((const typename FT::Ctx*)ctx)[g.key[item / LEN / g.d]];
+            sign_chain_one<FT>(g, kc, item);
+        }
+        return true;
+    }
+}
+
 // Batches of several parameter sets of one family (same F: LEN and n
-// agree, d, h', index and signature sizes may differ) in ONE launch over one
-// shared ticket counter.  Each batch's ticket sequence is cut into phases -
-// its key contexts, H_msg and h_pre, then one phase per layer - and the
-// shared sequence takes phase 0 of every batch, then layer 0 of every batch,
-// then layer 1 of the batches that have one, and so on (segment s = local
-// tickets [local0[s], local0[s] + first[s + 1] - first[s]) of batch job[s]).
-// Every batch keeps its own order and depends on nothing of the others, so
-// the sequence is still topological and the launch completes whatever the
-// residency, while the batches run their phases side by side.  A batch whose
-// dependency wait ran out (its own error flag) skips its remaining tickets
-// and ends with -3 in its statuses; the others finish.
+// agree; d, h', index and signature sizes may differ) and of all three
+// kinds in ONE launch over one shared ticket counter.  Each batch's ticket
+// sequence is cut into phases - a verify batch's key contexts, H_msg and
+// h_pre, then one phase per layer; a keygen or sign batch is one phase - and
+// the shared sequence takes phase 0 of every batch, then layer 0 of every
+// verify batch, then layer 1 of those that have one, and so on (segment s =
+// local tickets [local0[s], local0[s] + first[s + 1] - first[s]) of batch
+// job[s]).  Every batch keeps its own order and depends on nothing of the
+// others, so the sequence is still topological and the launch completes
+// whatever the residency, while the batches run their phases side by side.
+// A batch whose dependency wait ran out (its own error flag) skips its
+// remaining tickets; a verify batch then ends with -3 in its statuses, the
+// others finish.
 constexpr uint32_t kMaxPersistJobs = 8;
 constexpr uint32_t kMaxPersistSegs = kMaxPersistJobs * 13;  // phases: 1 + up to 12 layers
 struct PersistJobs {
-    VerifyArgs v[kMaxPersistJobs];
-    PersistArgs q[kMaxPersistJobs];
+    PersistBatch job[kMaxPersistJobs];
     unsigned long long first[kMaxPersistSegs + 1];  // first shared ticket of each segment
     unsigned long long local0[kMaxPersistSegs];     // its first ticket in its batch's sequence
-    uint8_t job[kMaxPersistSegs];                   // its batch
+    uint8_t seg_job[kMaxPersistSegs];               // its batch
     unsigned long long* ticket;  // the shared ticket counter (zeroed before the launch)
     uint32_t* exited;            // CTAs that have left the loop (zeroed before the launch)
     uint32_t njobs, nsegs;
 };
 
-template <class F, class FT>
+// GEN: the launch holds keygen or sign batches (their task code raises the
+// kernel's register use, so launches of verify batches only leave it out).
+template <class F, class FT, bool GEN>
 __global__ void __launch_bounds__(128, persist_min_ctas<F>())
     k_verify_persist_multi(const __grid_constant__ PersistJobs P)
 {
@@ -499,9 +730,14 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>())
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= total) break;
         while (t >= P.first[sg + 1]) sg++;
-        const uint32_t j = P.job[sg];
-        if (*(volatile uint32_t*)P.q[j].hdr) continue;  // that batch failed
-        persist_step<F, FT>(P.v[j], P.q[j], P.local0[sg] + (t - P.first[sg]), cnt);
+        const PersistBatch& J = P.job[P.seg_job[sg]];
+        if (*(volatile uint32_t*)J.q.hdr) continue;  // that batch failed
+        const unsigned long long lt = P.local0[sg] + (t - P.first[sg]);
+        if (!GEN || J.kind == kJobVerify) {
+            persist_step<F, FT>(J.v, J.q, lt, cnt);
+        } else if constexpr (GEN) {
+            gen_step<F, FT>(J, lt);
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -512,8 +748,8 @@ __global__ void __launch_bounds__(128, persist_min_ctas<F>())
     if (sh_last) {
         __threadfence();
         for (uint32_t k = 0; k < P.njobs; k++)
-            if (*(volatile uint32_t*)P.q[k].hdr)
-                for (uint32_t s = threadIdx.x; s < P.v[k].count; s += blockDim.x) P.v[k].status[s] = -3;
+            if (P.job[k].kind == kJobVerify && *(volatile uint32_t*)P.job[k].q.hdr)
+                for (uint32_t s = threadIdx.x; s < P.job[k].v.count; s += blockDim.x) P.job[k].v.status[s] = -3;
     }
 }
 

@@ -863,10 +863,8 @@ struct SignArgs {
 // authentication paths copied out of the subtree node arrays.
 // HMSG_DONE: R and layer 0's chain lengths were written by k_sign_hmsg_warp.
 template <class F, bool HMSG_DONE = false>
-__global__ void k_sign_prep(SignArgs g, const typename F::Ctx* __restrict__ ctx)
+__device__ __forceinline__ void sign_prep_one(const SignArgs& g, const typename F::Ctx* __restrict__ ctx, uint32_t s)
 {
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= g.count) return;
     uint8_t* sm = g.sm + g.sm_off[s];
     const uint64_t idx = g.idx[s];
     const uint32_t th = g.tree_height;
@@ -900,6 +898,13 @@ __global__ void k_sign_prep(SignArgs g, const typename F::Ctx* __restrict__ ctx)
     }
 }
 
+template <class F, bool HMSG_DONE = false>
+__global__ void k_sign_prep(SignArgs g, const typename F::Ctx* __restrict__ ctx)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < g.count) sign_prep_one<F, HMSG_DONE>(g, ctx, s);
+}
+
 // R and H_msg of each signature with one WARP per signature (kWarpHmsg
 // families: the warp-parallel permutation), writing R into the signature and
 // layer 0's chain lengths; k_sign_prep<F, true> does the rest.  Two
@@ -925,10 +930,8 @@ __global__ void __launch_bounds__(64) k_sign_hmsg_warp(SignArgs g, const typenam
 // One thread per (signature, layer, chain): PRF_keygen then gen_chain(0,
 // len_i) of wots_sign (wots.c:136-154).
 template <class F>
-__global__ void __launch_bounds__(128) k_sign_chains(SignArgs g, const typename F::Ctx* __restrict__ ctx)
+__device__ __forceinline__ void sign_chain_one(const SignArgs& g, const typename F::Ctx& c, uint64_t item)
 {
-    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (item >= (uint64_t)g.count * g.d * F::LEN) return;
     const uint64_t sl = item / F::LEN;
     const uint32_t chain = (uint32_t)(item - sl * F::LEN);
     const uint32_t s = (uint32_t)(sl / g.d);
@@ -938,13 +941,20 @@ __global__ void __launch_bounds__(128) k_sign_chains(SignArgs g, const typename 
     const uint32_t leaf = (uint32_t)((idx >> (th * layer)) & ((1ull << th) - 1));
     const uint64_t tree = (th * (layer + 1) >= 64) ? 0 : idx >> (th * (layer + 1));
     const uint32_t steps = g.lens[item];
-    const typename F::Ctx& c = ctx[g.key[s]];
     uint32_t x[F::NW], a[8];
     set_addr(a, layer, tree, ADDR_OTS, leaf, chain, 0);
     run_chain<F>(x, c, a, 0, steps, true);
     const uint64_t wsb = (uint64_t)F::LEN * F::N;
     uint8_t* sig = g.sm + g.sm_off[s] + g.index_bytes + F::N + layer * (wsb + (uint64_t)th * F::N);
     F::store(sig + (uint64_t)chain * F::N, x);
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) k_sign_chains(SignArgs g, const typename F::Ctx* __restrict__ ctx)
+{
+    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= (uint64_t)g.count * g.d * F::LEN) return;
+    sign_chain_one<F>(g, ctx[g.key[item / F::LEN / g.d]], item);
 }
 
 // ---------------------------------------------------------------------------

@@ -788,6 +788,7 @@ class BatchGroup(C.Structure):
 
 
 lib.xmss_b200_batch_create.argtypes = [C.POINTER(BatchGroup), C.c_uint32, C.POINTER(C.c_void_p)]
+lib.xmss_b200_batch_create_persistent.argtypes = lib.xmss_b200_batch_create.argtypes
 lib.xmss_b200_batch_launch.argtypes = [C.c_void_p, C.c_void_p]
 lib.xmss_b200_batch_destroy.argtypes = [C.c_void_p]
 lib.xmss_b200_batch_destroy.restype = None
@@ -799,7 +800,7 @@ class Batch:
     group's "sk" is a writable uint8 numpy array (count x (4 + sk_bytes)),
     advanced in place by create, and its codes land in self.ret[i]."""
 
-    def __init__(self, groups: Sequence[dict]):
+    def __init__(self, groups: Sequence[dict], persistent: bool = False):
         arr = (BatchGroup * len(groups))()
         self._keep = []
         self.ret = []
@@ -817,7 +818,8 @@ class Batch:
             for k, v in g.items():
                 setattr(arr[i], k, v)
         h = C.c_void_p()
-        r = _check(lib.xmss_b200_batch_create(arr, len(groups), C.byref(h)), "batch_create")
+        create = lib.xmss_b200_batch_create_persistent if persistent else lib.xmss_b200_batch_create
+        r = _check(create(arr, len(groups), C.byref(h)), "batch_create")
         if r:
             raise ValueError(f"batch_create returned {r}: {last_error()}")
         self._h = h

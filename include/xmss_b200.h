@@ -201,6 +201,17 @@ typedef struct {
 typedef struct xmss_b200_batch xmss_b200_batch;
 
 int xmss_b200_batch_create(const xmss_b200_batch_group *groups, uint32_t ngroups, xmss_b200_batch **out);
+/* The same batch as persistent launches fed by a device work queue: the
+ * groups of one hash family (keygen, sign and verify alike, any parameter
+ * sets, up to 8 per launch) run as ONE persistent kernel launch whose warps
+ * take the tasks of all of them from one ticket sequence (subtree chains,
+ * L-tree levels and Merkle levels, key output, signature preparation and
+ * chains, and the verify tasks of xmss_b200_sign_open_device_persistent),
+ * the families' launches concurrent on forked streams, all captured in one
+ * CUDA graph.  Same results, rules and return codes as
+ * xmss_b200_batch_create. */
+int xmss_b200_batch_create_persistent(const xmss_b200_batch_group *groups, uint32_t ngroups,
+                                      xmss_b200_batch **out);
 int xmss_b200_batch_launch(xmss_b200_batch *b, void *stream);
 void xmss_b200_batch_destroy(xmss_b200_batch *b);
 

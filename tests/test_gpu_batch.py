@@ -46,7 +46,11 @@ def _keygen_expect(oracle, po, seed):
     return root + seed[2 * n:], bytes(po.index_bytes) + seed[:2 * n] + root + seed[2 * n:]
 
 
-def test_mixed_batch_one_graph_matches_oracle(xb, oracle):
+@pytest.mark.parametrize("persistent", [False, True])
+def test_mixed_batch_one_graph_matches_oracle(xb, oracle, persistent):
+    """persistent: the same batch as one persistent launch per hash family
+    (xmss_b200_batch_create_persistent: keygen, sign and verify tasks of
+    every set of the family in one device work queue)."""
     torch = pytest.importorskip("torch")
     rng = np.random.default_rng(zlib.crc32(b"mixed batch"))
     groups, checks, keep = [], [], []
@@ -118,7 +122,7 @@ def test_mixed_batch_one_graph_matches_oracle(xb, oracle):
         want = [oracle.sign_open(po, s, bytes(pks[k, 4:]))[0] for s, k in zip(sms, vkey)]
         checks.append(("verify", po, want, d_st))
     torch.cuda.synchronize()
-    b = xb.Batch(groups)
+    b = xb.Batch(groups, persistent=persistent)
     # create signed nothing into the caller's buffers
     for c in checks:
         if c[0] == "sign":
@@ -157,7 +161,8 @@ def test_mixed_batch_one_graph_matches_oracle(xb, oracle):
     b.close()
 
 
-def test_keygen_verify_batch_relaunches(xb, oracle):
+@pytest.mark.parametrize("persistent", [False, True])
+def test_keygen_verify_batch_relaunches(xb, oracle, persistent):
     """A batch without sign groups replays: refilled buffers give new results
     at each launch (keygen from new seeds, verify statuses rewritten)."""
     torch = pytest.importorskip("torch")
@@ -183,7 +188,7 @@ def test_keygen_verify_batch_relaunches(xb, oracle):
                        d_sk=d_sk.data_ptr()),
                   dict(kind=xb.VERIFY, oid=1, mt=0, count=8, d_sm=d_sm.data_ptr(), d_sm_off=d_off.data_ptr(),
                        d_len=d_len.data_ptr(), d_pk=d_vpk.data_ptr(), npk=1, d_pk_index=d_ix.data_ptr(),
-                       d_status=d_st.data_ptr())])
+                       d_status=d_st.data_ptr())], persistent=persistent)
     for rep in range(2):
         seeds = np.frombuffer(rng.bytes(4 * 3 * n), np.uint8).reshape(4, 3 * n)
         d_seeds.copy_(torch.from_numpy(seeds.copy()))
