@@ -535,6 +535,30 @@ __host__ __device__ inline unsigned long long gen_total(const PersistBatch& J, i
     return c[0] + c[1] + c[2] + c[3] + c[4] + c[5];
 }
 
+// The rare, register-heavy tasks of a keygen or sign batch, kept out of
+// line so that the chain loop of the frequent tasks keeps its registers.
+template <class F>
+__device__ __noinline__ void gen_ctx_task(const TreeTask& T, typename F::Ctx* ctx, uint32_t k)
+{
+    if (k < T.nkeys) {
+        const uint8_t* row = T.keys + (uint64_t)k * T.key_stride;
+        typename F::Ctx x;
+        F::make_ctx(x, row + T.off_pub, row + T.off_sks, row + T.off_skp);
+        ctx[k] = x;
+    }
+}
+
+template <class F>
+__device__ __noinline__ void gen_sign_prep_task(const SignArgs& g, const TreeTask& T, const typename F::Ctx* ctx,
+                                                uint32_t s)
+{
+    if (s < g.count) {
+        sign_prep_one<F>(g, ctx, s);
+        uint8_t* sm = g.sm + g.sm_off[s];
+        for (uint32_t i = 0; i < g.index_bytes; i++) sm[i] = T.ibytes[(uint64_t)s * 8 + i];
+    }
+}
+
 // Runs ticket t of a keygen or sign batch (whole warp); false when a wait
 // ran out or the batch failed.
 template <class F, class FT>
@@ -550,13 +574,7 @@ __device__ __forceinline__ bool gen_step(const PersistBatch& J, unsigned long lo
     unsigned long long c[6];
     gen_counts(J, LEN, c);
     if (t < c[0]) {  // -------- contexts of 32 keys
-        const uint32_t k = (uint32_t)t * 32 + lane;
-        if (k < T.nkeys) {
-            const uint8_t* row = T.keys + (uint64_t)k * T.key_stride;
-            Ctx x;
-            F::make_ctx(x, row + T.off_pub, row + T.off_sks, row + T.off_skp);
-            ctx[k] = x;
-        }
+        gen_ctx_task<F>(T, ctx, (uint32_t)t * 32 + lane);
         persist_signal(&q.hdr[2]);
         return true;
     }
@@ -665,12 +683,7 @@ __device__ __forceinline__ bool gen_step(const PersistBatch& J, unsigned long lo
     const SignArgs& g = J.g;
     if (t < c[4]) {  // -------- preparation of 32 signatures (every subtree built)
         if (!persist_wait(T.trees_done, T.ntrees, err, q.wait_ns)) return false;
-        const uint32_t s = (uint32_t)t * 32 + lane;
-        if (s < g.count) {
-            sign_prep_one<F>(g, ctx, s);
-            uint8_t* sm = g.sm + g.sm_off[s];
-            for (uint32_t i = 0; i < g.index_bytes; i++) sm[i] = T.ibytes[(uint64_t)s * 8 + i];
-        }
+        gen_sign_prep_task<F>(g, T, ctx, (uint32_t)t * 32 + lane);
         persist_signal(T.prep_done);
         return true;
     }
@@ -712,10 +725,18 @@ struct PersistJobs {
     uint32_t njobs, nsegs;
 };
 
-// GEN: the launch holds keygen or sign batches (their task code raises the
-// kernel's register use, so launches of verify batches only leave it out).
+// GEN: the launch holds keygen or sign batches.  Their task code raises the
+// kernel's register use, so launches of verify batches only leave it out,
+// and with it the SHA-256 form runs 4 CTAs per SM (128 registers, ~0.5 KB of
+// spills) instead of 5 (96 registers, ~1 KB).
+template <class F>
+constexpr int persist_gen_min_ctas()
+{
+    return persist_min_ctas<F>() > 2 ? persist_min_ctas<F>() - 1 : persist_min_ctas<F>();
+}
+
 template <class F, class FT, bool GEN>
-__global__ void __launch_bounds__(128, persist_min_ctas<F>())
+__global__ void __launch_bounds__(128, GEN ? persist_gen_min_ctas<F>() : persist_min_ctas<F>())
     k_verify_persist_multi(const __grid_constant__ PersistJobs P)
 {
     __shared__ uint32_t sh_cnt[4][32];
