@@ -69,6 +69,8 @@ def _device_statuses(xb, torch, entry, oid, mt, buf, off, ln, pks, keyix, calls=
     ("XMSS-SHA2_10_256", 1),
     ("XMSS-SHA2_10_256", 33),
     ("XMSS-SHA2_10_256", 250),
+    ("XMSS-SHA2_10_256", 1100),
+    ("XMSSMT-SHA2_20/2_256", 1030),
     ("XMSS-SHA2_10_512", 70),
     ("XMSS-SHAKE_10_256", 70),
     ("XMSS-SHAKE_10_512", 40),
