@@ -129,13 +129,13 @@ struct Launch {
                 return;
             }
             const uint32_t hb = (v.count + 63) / 64;
-            k_verify_prep<F><<<hb, 64, 0, st>>>(v, hb, (const Ctx*)ctx);
+            k_verify_prep<F, 1><<<hb, 64, 0, st>>>(v, hb, (const Ctx*)ctx);
             return;
         }
         // the h_pre blocks alone (the chain kernels' pipe mix and 128-thread
         // CTAs measured slower here)
         const uint64_t pre = (uint64_t)v.count * v.d * (F::LEN - 1 + v.tree_height);
-        k_verify_prep<F><<<grid_for(pre, 64), 64, 0, st>>>(v, 0, (const Ctx*)ctx);
+        k_verify_prep<F, 2><<<grid_for(pre, 64), 64, 0, st>>>(v, 0, (const Ctx*)ctx);
     }
     static void verify_scatter(const VerifyArgs& v, uint32_t layer, cudaStream_t st)
     {

@@ -475,13 +475,15 @@ __device__ __forceinline__ void verify_hpre_item(const VerifyArgs& v, const type
 }
 
 // Launch = [hmsg_blocks x 64 threads: one signature each] followed by
-// [pre blocks: one H node's h_pre each]; either part may be empty.
-template <class F>
+// [pre blocks: one H node's h_pre each]; either part may be empty.  PART 1
+// and 2 compile only the H_msg or only the h_pre path (the launches of a
+// split batch): each gets its own register allocation and a smaller body.
+template <class F, int PART = 0>
 __global__ void __launch_bounds__(64) k_verify_prep(VerifyArgs v, uint32_t hmsg_blocks_n,
                                                     const typename F::Ctx* __restrict__ ctx)
 {
     __shared__ uint32_t sh_hist[16];
-    if (blockIdx.x < hmsg_blocks_n) {
+    if (PART != 2 && (PART == 1 || blockIdx.x < hmsg_blocks_n)) {
         if (threadIdx.x < 16) sh_hist[threadIdx.x] = 0;
         __syncthreads();
         const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -513,7 +515,8 @@ __global__ void __launch_bounds__(64) k_verify_prep(VerifyArgs v, uint32_t hmsg_
         flush_hist(sh_hist, v.hist);
         return;
     }
-    verify_hpre_item<F>(v, ctx, (uint64_t)(blockIdx.x - hmsg_blocks_n) * blockDim.x + threadIdx.x);
+    if constexpr (PART != 1)
+        verify_hpre_item<F>(v, ctx, (uint64_t)(blockIdx.x - hmsg_blocks_n) * blockDim.x + threadIdx.x);
 }
 
 // The H_msg part of k_verify_prep with one WARP per signature, for the
