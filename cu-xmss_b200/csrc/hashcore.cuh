@@ -240,6 +240,140 @@ __device__ __forceinline__ void sha256_iv(uint32_t (&st)[8])
     st[4] = 0x510e527fu; st[5] = 0x9b05688cu; st[6] = 0x1f83d9abu; st[7] = 0x5be0cd19u;
 }
 
+// ---------------------------------------------------------------------------
+// SHA-256 on state slots, for compressions that resume after a known prefix of
+// rounds.  Role r (0 = a, ..., 7 = h) of round t lives in slot (r - t) & 7, so
+// a round rewrites two slots and moves nothing, and the slots after any round
+// can be stored and resumed from.  Round and schedule arithmetic are those of
+// sha256_compress_t<MIX> (MIX 0, 1, 2).
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr uint32_t sha256_k(int t)
+{
+    constexpr uint32_t K[64] = {
+        0x428a2f98u, 0x71374491u, 0xb5c0fbcfu, 0xe9b5dba5u, 0x3956c25bu, 0x59f111f1u,
+        0x923f82a4u, 0xab1c5ed5u, 0xd807aa98u, 0x12835b01u, 0x243185beu, 0x550c7dc3u,
+        0x72be5d74u, 0x80deb1feu, 0x9bdc06a7u, 0xc19bf174u, 0xe49b69c1u, 0xefbe4786u,
+        0x0fc19dc6u, 0x240ca1ccu, 0x2de92c6fu, 0x4a7484aau, 0x5cb0a9dcu, 0x76f988dau,
+        0x983e5152u, 0xa831c66du, 0xb00327c8u, 0xbf597fc7u, 0xc6e00bf3u, 0xd5a79147u,
+        0x06ca6351u, 0x14292967u, 0x27b70a85u, 0x2e1b2138u, 0x4d2c6dfcu, 0x53380d13u,
+        0x650a7354u, 0x766a0abbu, 0x81c2c92eu, 0x92722c85u, 0xa2bfe8a1u, 0xa81a664bu,
+        0xc24b8b70u, 0xc76c51a3u, 0xd192e819u, 0xd6990624u, 0xf40e3585u, 0x106aa070u,
+        0x19a4c116u, 0x1e376c08u, 0x2748774cu, 0x34b0bcb5u, 0x391c0cb3u, 0x4ed8aa4au,
+        0x5b9cca4fu, 0x682e6ff3u, 0x748f82eeu, 0x78a5636fu, 0x84c87814u, 0x8cc70208u,
+        0x90befffau, 0xa4506cebu, 0xbef9a3f7u, 0xc67178f2u};
+    return K[t];
+}
+
+// W[t] for t >= 16 into the 16-word window (FIPS 180-4 6.2.2 step 1).
+template <int MIX>
+__device__ __forceinline__ void sha256_sched(uint32_t (&w)[16], int t)
+{
+    const uint32_t x15 = w[(t - 15) & 15], x2 = w[(t - 2) & 15];
+    if constexpr (MIX == 0) {
+        const uint32_t s0 = ror32(x15, 7) ^ ror32(x15, 18) ^ (x15 >> 3);
+        const uint32_t s1 = ror32(x2, 17) ^ ror32(x2, 19) ^ (x2 >> 10);
+        w[t & 15] += s0 + w[(t - 7) & 15] + s1;
+    } else {
+        const uint32_t r0 = (MIX == 2) ? fma_shr<3>(x15) : (x15 >> 3);
+        const uint32_t r1 = (MIX == 2) ? fma_shr<10>(x2) : (x2 >> 10);
+        const uint32_t s0 = ror32(x15, 7) ^ ror32(x15, 18) ^ r0;
+        const uint32_t s1 = ror32(x2, 17) ^ ror32(x2, 19) ^ r1;
+        w[t & 15] = fma_add(s1, fma_add(s0, w[t & 15] + w[(t - 7) & 15]));
+    }
+}
+
+// Round t on slots (t must be a constant after unrolling).
+template <int MIX>
+__device__ __forceinline__ void sha256_round_s(uint32_t (&s)[8], int t, uint32_t wt)
+{
+    const uint32_t a = s[(0 - t) & 7], b = s[(1 - t) & 7], c = s[(2 - t) & 7];
+    const uint32_t e = s[(4 - t) & 7], f = s[(5 - t) & 7], g = s[(6 - t) & 7];
+    uint32_t& d = s[(3 - t) & 7];
+    uint32_t& h = s[(7 - t) & 7];
+    const uint32_t S1 = ror32(e, 6) ^ ror32(e, 11) ^ ror32(e, 25);
+    const uint32_t ch = g ^ (e & (f ^ g));
+    const uint32_t S0 = ror32(a, 2) ^ ror32(a, 13) ^ ror32(a, 22);
+    const uint32_t mj = (a & b) | (c & (a | b));
+    if constexpr (MIX == 0) {
+        const uint32_t t1 = h + S1 + ch + sha256_k(t) + wt;
+        d += t1;
+        h = t1 + S0 + mj;
+    } else {
+        const uint32_t t1 = fma_add(ch, fma_add(S1, h + sha256_k(t) + wt));
+        d = fma_add(d, t1);
+        h = fma_add(S0, fma_add(mj, t1));
+    }
+}
+
+// The slots after rounds 0..7 from the IV with W0..W7 = 0: the first block of
+// every hash whose input starts with toByte(0, 32) (thash_f's core block).
+struct Sha256Slots {
+    uint32_t v[8];
+};
+__host__ __device__ constexpr uint32_t sha256_ror_c(uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
+__host__ __device__ constexpr Sha256Slots sha256_zero_prefix8()
+{
+    Sha256Slots s{{0x6a09e667u, 0xbb67ae85u, 0x3c6ef372u, 0xa54ff53au, 0x510e527fu, 0x9b05688cu, 0x1f83d9abu,
+                   0x5be0cd19u}};
+    for (int t = 0; t < 8; t++) {
+        const uint32_t a = s.v[(0 - t) & 7], b = s.v[(1 - t) & 7], c = s.v[(2 - t) & 7];
+        const uint32_t e = s.v[(4 - t) & 7], f = s.v[(5 - t) & 7], g = s.v[(6 - t) & 7];
+        const uint32_t S1 = sha256_ror_c(e, 6) ^ sha256_ror_c(e, 11) ^ sha256_ror_c(e, 25);
+        const uint32_t S0 = sha256_ror_c(a, 2) ^ sha256_ror_c(a, 13) ^ sha256_ror_c(a, 22);
+        const uint32_t t1 = s.v[(7 - t) & 7] + S1 + (g ^ (e & (f ^ g))) + sha256_k(t);
+        s.v[(3 - t) & 7] += t1;
+        s.v[(7 - t) & 7] = t1 + S0 + ((a & b) | (c & (a | b)));
+    }
+    return s;
+}
+
+// A 32-bit shared-memory load the compiler keeps where it is written (not
+// hoisted out of a loop into registers that would stay live across it).
+__device__ __forceinline__ uint32_t lds_u32(const uint32_t* p)
+{
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"((uint32_t)__cvta_generic_to_shared(p)));
+    return v;
+}
+
+// The rounds of one compression resumed from slots s; on return s holds the
+// final slots and the caller adds its chaining value (the feed-forward):
+//   skip 0  s = the chaining value, rounds 0..63;
+//   skip 6  s = the slots after rounds 0..5, and the shared-memory words
+//           pre[0], pre[stride], ..., pre[4 * stride] = W16..W20 (which read
+//           only W0..W5 and W9..W15);
+//   skip 8  s = the slots after rounds 0..7 (w[0..7] still hold W0..W7).
+// `skip` must be the same for every thread of a warp (a branch, not a select).
+template <int MIX>
+__device__ __forceinline__ void sha256_rounds_resume(uint32_t (&s)[8], uint32_t (&w)[16], int skip,
+                                                     const uint32_t* pre, int stride)
+{
+    if (skip == 0) {
+#pragma unroll
+        for (int t = 0; t < 6; t++) sha256_round_s<MIX>(s, t, w[t]);
+    }
+    if (skip != 8) {
+#pragma unroll
+        for (int t = 6; t < 8; t++) sha256_round_s<MIX>(s, t, w[t]);
+    }
+#pragma unroll
+    for (int t = 8; t < 16; t++) sha256_round_s<MIX>(s, t, w[t]);
+    if (skip == 6) {
+#pragma unroll
+        for (int t = 16; t < 21; t++) w[t & 15] = lds_u32(pre + (t - 16) * stride);
+    } else {
+#pragma unroll
+        for (int t = 16; t < 21; t++) sha256_sched<MIX>(w, t);
+    }
+#pragma unroll
+    for (int t = 16; t < 21; t++) sha256_round_s<MIX>(s, t, w[t & 15]);
+#pragma unroll
+    for (int t = 21; t < 64; t++) {
+        sha256_sched<MIX>(w, t);
+        sha256_round_s<MIX>(s, t, w[t & 15]);
+    }
+}
+
 // SHA-256 of a message of MW big-endian words (4*MW bytes), from the IV.
 template <int MW>
 __device__ __forceinline__ void sha256_words(uint32_t (&out)[8], const uint32_t (&m)[MW])
