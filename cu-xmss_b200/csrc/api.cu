@@ -504,13 +504,14 @@ namespace {
 
 // Buffers of one caller stream for xmss_b200_sign_open_batch_async: scratch
 // and staging that grow stream-ordered on that stream, a second stream for
-// the split of large batches, and the end of the stream's last call.
+// the split of large batches, and the point where the stream's last call
+// has copied its pinned staging to the device.
 struct StreamCtx {
     xb::SplitStreams split;
     xb::Workspace w;
     xb::DevBuf d;
     xb::PinnedBuf h;
-    cudaEvent_t done = nullptr;
+    cudaEvent_t staged = nullptr;
     bool pending = false;
 };
 
@@ -526,7 +527,7 @@ StreamCtx& stream_ctx(cudaStream_t st)
         n->h.keep_old_blocks();
         n->split.create();
         n->w.split = &n->split;
-        XB_CUDA(cudaEventCreateWithFlags(&n->done, cudaEventDisableTiming));
+        XB_CUDA(cudaEventCreateWithFlags(&n->staged, cudaEventDisableTiming));
         c = std::move(n);
     }
     return *c;
@@ -554,8 +555,10 @@ extern "C" int xmss_b200_sign_open_batch_async(int mt, uint32_t count, const uin
         cudaStream_t st = (cudaStream_t)stream;
         XB_CUDA(cudaSetDevice(e.device()));
         StreamCtx& c = stream_ctx(st);
-        // the stream's previous call must be past its staging
-        if (c.pending) XB_CUDA(cudaEventSynchronize(c.done));
+        // The staging block is rewritten below, so the stream's previous call
+        // must have copied it to the device; its kernels and its status copy
+        // may still be queued (the device buffers are reused in stream order).
+        if (c.pending) XB_CUDA(cudaEventSynchronize(c.staged));
         uint64_t raw = 0;
         for (uint32_t i = 0; i < count; i++) raw = std::max(raw, sm_off[i] + smlen[i]);
         const uint64_t span = (raw + 15) & ~15ull;
@@ -575,12 +578,12 @@ extern "C" int xmss_b200_sign_open_batch_async(int mt, uint32_t count, const uin
         uint8_t* d = c.d.as<uint8_t>(total);
         if (raw) XB_CUDA(cudaMemcpyAsync(d, sm, raw, cudaMemcpyHostToDevice, st));
         XB_CUDA(cudaMemcpyAsync(d + o_off, h, o_st - o_off, cudaMemcpyHostToDevice, st));
+        XB_CUDA(cudaEventRecord(c.staged, st));
+        c.pending = true;
         e.verify(ops, p, count, d, (const uint64_t*)(d + o_off), (const uint64_t*)(d + o_len), d + o_pk, npk,
                  (const uint32_t*)(d + o_idx), (int*)(d + o_st), st, c.w, true);
         XB_CUDA(cudaMemcpyAsync(status, d + o_st, count * 4, cudaMemcpyDeviceToHost, st));
         XB_CUDA(cudaGetLastError());
-        XB_CUDA(cudaEventRecord(c.done, st));
-        c.pending = true;
         return kOk;
     });
 }

@@ -124,8 +124,10 @@ int xmss_b200_set_wait_bound(unsigned long long ns);
  * passed this call (cudaStreamSynchronize or an event).  sm_off, smlen, pk
  * and pk_index are read before the call returns.  Each stream has its own
  * device buffers, so calls on two or more streams overlap one batch's
- * copies with another's kernels; a call waits for the previous call on the
- * same stream to finish first.  No reference counterpart beyond the
+ * copies with another's kernels.  A call waits (on the host) only until the
+ * previous call on the same stream has copied its inputs to the device;
+ * calls on one stream then run one after another on the GPU, so a caller can
+ * queue several batches ahead.  No reference counterpart beyond the
  * xmss[mt]_sign_open calls it batches (xmss.c:45-60, 95-109). */
 int xmss_b200_sign_open_batch_async(int mt, uint32_t count, const uint8_t *sm, const uint64_t *sm_off,
                                     const uint64_t *smlen, const uint8_t *pk, uint32_t npk,

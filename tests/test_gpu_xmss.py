@@ -344,6 +344,30 @@ def test_sign_open_batch_async_two_streams(xb, oracle):
     assert (outs[0] == want).all() and (outs[1] == want).all()
     assert (outs[2][:300] == want[:300]).all() and (outs[3][:300] == want[:300]).all()
 
+    # Calls queued ahead: a call waits only until the previous call on its
+    # stream has copied its inputs, so several batches per stream are in
+    # flight at once; small and large batches alternate, so a stream's
+    # buffers grow while its earlier calls are still queued, and the host
+    # arrays are rewritten between calls (they are read before a call
+    # returns).
+    plan = [slice(700, 1000), slice(0, count), slice(100, 250), slice(0, count), slice(1200, 1500), slice(0, count)]
+    outs = [torch.full((count,), 7, dtype=torch.int32).pin_memory().numpy() for _ in range(2 * len(plan))]
+    streams = [torch.cuda.Stream() for _ in range(2)]
+    h_off, h_len, h_kix = off.copy(), ln.copy(), keyix.copy()
+    for i, o in enumerate(outs):
+        s = plan[i % len(plan)]
+        n = s.stop - s.start
+        h_off[:n], h_len[:n], h_kix[:n] = off[s], ln[s], keyix[s]
+        xb.sign_open_batch_async(False, h_sm, np.ascontiguousarray(h_off[:n]), np.ascontiguousarray(h_len[:n]),
+                                 pks, np.ascontiguousarray(h_kix[:n]), o, streams[i % 2].cuda_stream)
+        h_off[:] = 0  # reuse of the host arrays after the call returned
+    torch.cuda.synchronize()
+    for i, o in enumerate(outs):
+        s = plan[i % len(plan)]
+        n = s.stop - s.start
+        assert (o[:n] == want[s]).all(), i
+        assert (o[n:] == 7).all(), i
+
 
 @pytest.mark.parametrize("count", [300, 1100])
 def test_verify_graph_replays(xb, count):
