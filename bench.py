@@ -520,6 +520,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         os.sched_setaffinity(0, cpus_before)  # the CPU baseline uses every host core
     if rank == 0 and world == 1 and not args.skip_cpu:
         cpu = cpu_baseline(w, budget_s=args.cpu_seconds)
+        if "keygen" in sec:
+            sec["keygen"]["cpu_baseline"] = cpu_keygen_baseline(xb)
 
     if rank != 0:
         return None
@@ -769,6 +771,44 @@ def cpu_baseline(w, budget_s: float = 2.5, sample=None, pool=None):
     return {"value": done / dt, "unit": "verifies/s", "cores": cores, "kind": kind,
             "sample": f"{done} verifies ({len(sms)}-signature sample of the same workload, repeated) "
                       f"in {dt:.2f} s on {cores} processes", "correct": ok}
+
+
+def _cpu_keygen_one(seed: bytes):
+    """One XMSS-SHA2_10_256 keypair (1,024 leaves) from `seed` with the
+    reference build (oracle/_ref; the oracle's restatement where it is
+    absent): its public key and seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import REF_PATH, Oracle, RefLib
+
+    lib = RefLib() if os.path.exists(REF_PATH) else Oracle()
+    p = lib.params(0x01)
+    t0 = time.perf_counter()
+    pk, _ = lib.seed_keypair(p, seed)
+    return pk, time.perf_counter() - t0, "reference" if os.path.exists(REF_PATH) else "port"
+
+
+def cpu_keygen_baseline(xb):
+    """Reference CPU keygen leaves/s on all host cores: one XMSS-SHA2_10_256
+    keypair per core (xmssmt_core_seed_keypair, cuxmss/xmss_core.c:134-161),
+    one spawned process each.  A leaf costs the same 4,550 compressions at
+    every tree height, so leaves/s compares with the h = 16 / h = 20 keygen.
+    The public keys are compared with this library's keys of the same seeds."""
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(SEED + 17)
+    seeds = [rng.bytes(96) for _ in range(cores)]
+    with mp.get_context("spawn").Pool(cores) as pool:
+        pool.map(abs, range(cores))  # workers started before the clock
+        t0 = time.perf_counter()
+        res = pool.map(_cpu_keygen_one, seeds, chunksize=1)
+        dt = time.perf_counter() - t0
+    pks, _ = xb.keypair_batch(0x01, False, np.frombuffer(b"".join(seeds), np.uint8).reshape(cores, 96))
+    correct = all(bytes(pks[i][4:]) == res[i][0] for i in range(cores))
+    return {"value": cores * 1024 / dt, "unit": "leaves/s", "cores": cores, "kind": res[0][2],
+            "sample": f"{cores} XMSS-SHA2_10_256 keys of 1,024 leaves, one per process, in {dt:.2f} s "
+                      f"(per key {min(r[1] for r in res):.2f}-{max(r[1] for r in res):.2f} s)",
+            "correct": correct}
 
 
 def run_reference(args, rank: int, world: int):
