@@ -66,10 +66,24 @@ __device__ __forceinline__ uint32_t fetch4_le(const uint8_t* m, uint64_t mlen, u
     return v;
 }
 
-// NW little-endian words from bytes at p (any alignment).
+// NW little-endian words from bytes at p (any alignment; 16-byte vector
+// loads where p is 16-byte aligned, as n-byte nodes of the node arrays are).
 template <int NW>
 __device__ __forceinline__ void load_le(uint32_t (&v)[NW], const uint8_t* p)
 {
+    if constexpr (NW % 4 == 0) {
+        if (((uintptr_t)p & 15) == 0) {
+#pragma unroll
+            for (int i = 0; i < NW; i += 4) {
+                const uint4 q = *(const uint4*)(p + 4 * i);
+                v[i] = q.x;
+                v[i + 1] = q.y;
+                v[i + 2] = q.z;
+                v[i + 3] = q.w;
+            }
+            return;
+        }
+    }
     if (((uintptr_t)p & 3) == 0) {
 #pragma unroll
         for (int i = 0; i < NW; i++) v[i] = ((const uint32_t*)p)[i];
