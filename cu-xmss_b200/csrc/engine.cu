@@ -802,7 +802,6 @@ void Engine::sign(const FamilyOps* ops, const xmss_params& p, uint32_t count, co
     ops->make_ctx(sp.keys + 3 * n, 4 * n, sp.keys, 4 * n, sp.keys + n, 4 * n, sp.nkeys, ctx, st);
     const uint64_t tree_bytes = ((2ull << th) - 1) * n;
     uint8_t* nodes = w.nodes.as<uint8_t>(sp.njobs * tree_bytes);
-    build_trees(ops, sp.jobs, sp.njobs, (int)th, nodes, ctx, st, w, subtree_k(p, sp.njobs));
     SignArgs g;
     g.sm = d_sm;
     g.sm_off = d_sm_off;
@@ -821,9 +820,25 @@ void Engine::sign(const FamilyOps* ops, const xmss_params& p, uint32_t count, co
     g.sig_bytes = p.sig_bytes;
     g.tree_height = th;
     g.d = d;
-    mark(kRoot, true, st);
-    ops->sign_prep(g, ctx, st);
-    mark(kRoot, false, st);
+    // R and H_msg read only the key contexts and the messages: they run on
+    // a second stream beside the subtree builds (a 64 KB message is ~1,000
+    // compressions in a row), and the rest of the preparation waits for both.
+    // The profiling pass keeps one sequence so each kernel's time is its own.
+    SplitStreams* ss = &w == &ws_ ? &split_ : w.split;
+    if (ss && !profiling) {
+        XB_CUDA(cudaEventRecord(ss->fork, st));
+        XB_CUDA(cudaStreamWaitEvent(ss->aux, ss->fork, 0));
+        ops->sign_hmsg(g, ctx, ss->aux);
+        XB_CUDA(cudaEventRecord(ss->join, ss->aux));
+        build_trees(ops, sp.jobs, sp.njobs, (int)th, nodes, ctx, st, w, subtree_k(p, sp.njobs));
+        XB_CUDA(cudaStreamWaitEvent(st, ss->join, 0));
+        ops->sign_prep_rest(g, ctx, st);
+    } else {
+        build_trees(ops, sp.jobs, sp.njobs, (int)th, nodes, ctx, st, w, subtree_k(p, sp.njobs));
+        mark(kRoot, true, st);
+        ops->sign_prep(g, ctx, st);
+        mark(kRoot, false, st);
+    }
     mark(kChains, true, st);
     ops->sign_chains(g, ctx, st);
     mark(kChains, false, st);

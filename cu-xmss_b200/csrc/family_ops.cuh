@@ -222,6 +222,23 @@ struct Launch {
         }
         k_sign_prep<F><<<(g.count + 63) / 64, 64, 0, st>>>(g, (const Ctx*)ctx);
     }
+    // sign_prep in two parts: R, H_msg and layer 0's chain lengths (needs no
+    // subtree), then the other layers' chain lengths and the authentication
+    // paths (needs the subtrees)
+    static void sign_hmsg(const SignArgs& g, const void* ctx, cudaStream_t st)
+    {
+        if (!g.count) return;
+        if constexpr (kWarpHmsg<F>) {
+            k_sign_hmsg_warp<F><<<(g.count + 1) / 2, 64, 0, st>>>(g, (const Ctx*)ctx);
+            return;
+        }
+        k_sign_hmsg<F><<<(g.count + 63) / 64, 64, 0, st>>>(g, (const Ctx*)ctx);
+    }
+    static void sign_prep_rest(const SignArgs& g, const void* ctx, cudaStream_t st)
+    {
+        if (!g.count) return;
+        k_sign_prep<F, true><<<(g.count + 63) / 64, 64, 0, st>>>(g, (const Ctx*)ctx);
+    }
     static void sign_chains(const SignArgs& g, const void* ctx, cudaStream_t st)
     {
         const uint64_t items = (uint64_t)g.count * g.d * F::LEN;
@@ -262,6 +279,8 @@ struct Launch {
         o.verify_persist = verify_persist;
         o.verify_persist_multi = verify_persist_multi;
         o.sign_prep = sign_prep;
+        o.sign_hmsg = sign_hmsg;
+        o.sign_prep_rest = sign_prep_rest;
         o.sign_chains = sign_chains;
         o.core_hash = core_hash;
         return o;

@@ -52,6 +52,10 @@ struct FamilyOps {
     // several batches of this family's parameter sets as one persistent launch
     void (*verify_persist_multi)(const PersistJobs& jobs, cudaStream_t st);
     void (*sign_prep)(const SignArgs& g, const void* ctx, cudaStream_t st);
+    // sign_prep's two parts: R, H_msg, layer 0's chain lengths (no subtree
+    // needed); the other layers' chain lengths and the authentication paths
+    void (*sign_hmsg)(const SignArgs& g, const void* ctx, cudaStream_t st);
+    void (*sign_prep_rest)(const SignArgs& g, const void* ctx, cudaStream_t st);
     void (*sign_chains)(const SignArgs& g, const void* ctx, cudaStream_t st);
     void (*core_hash)(const uint8_t* msgs, const uint64_t* off, const uint64_t* len, uint32_t count, uint8_t* out,
                       cudaStream_t st);

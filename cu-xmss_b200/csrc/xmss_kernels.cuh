@@ -908,6 +908,26 @@ __global__ void k_sign_prep(SignArgs g, const typename F::Ctx* __restrict__ ctx)
     if (s < g.count) sign_prep_one<F, HMSG_DONE>(g, ctx, s);
 }
 
+// R and H_msg of each signature with one thread per signature (the
+// families without a warp-parallel H_msg), writing R into the signature and
+// layer 0's chain lengths; k_sign_prep<F, true> does the rest.  It reads
+// only the key contexts, the key roots and the message, so it can run
+// beside the subtree builds.
+template <class F>
+__global__ void k_sign_hmsg(SignArgs g, const typename F::Ctx* __restrict__ ctx)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.count) return;
+    uint8_t* sm = g.sm + g.sm_off[s];
+    const uint64_t idx = g.idx[s];
+    uint32_t R[F::NW], root[F::NW], mh[F::NW];
+    F::prf_r(R, ctx[g.key[s]], idx);
+    F::store(sm + g.index_bytes, R);
+    F::load(root, g.key_root + (uint64_t)g.key[s] * g.key_stride);
+    hmsg<F>(mh, R, root, idx, g.msg ? g.msg + g.msg_off[s] : sm + g.sig_bytes, g.mlen[s]);
+    chain_lengths<F>(g.lens + ((uint64_t)s * g.d) * F::LEN, mh);
+}
+
 // R and H_msg of each signature with one WARP per signature (kWarpHmsg
 // families: the warp-parallel permutation), writing R into the signature and
 // layer 0's chain lengths; k_sign_prep<F, true> does the rest.  Two
