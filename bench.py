@@ -509,7 +509,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if world == 1 and not args.skip_keygen:
         sec["keygen"] = keygen_rate(xb, torch, dev, sh)
     if world == 1 and not args.skip_mix:
-        sec["mix"] = mix_rates(xb, torch, dev, sh)
+        sec["mix"] = mix_rates(xb, torch, dev, sh, cpu=not args.skip_cpu)
     if world == 1 and not args.skip_batch:
         sec["batch"] = batch_rates(xb, torch, dev, sh)
     if world == 1 and not args.skip_serve:
@@ -794,6 +794,48 @@ def _cpu_keygen_one(seed: bytes):
     return pk, time.perf_counter() - t0, "reference" if os.path.exists(REF_PATH) else "port"
 
 
+def _cpu_sign_one(job):
+    """One signature with the reference build (oracle/_ref; the oracle's
+    restatement where it is absent): job = (oid, mt, sk without the OID
+    prefix, message); the signed message and seconds."""
+    oid, mt, sk, msg = job
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import REF_PATH, Oracle, RefLib
+
+    lib = RefLib() if os.path.exists(REF_PATH) else Oracle()
+    p = lib.params(oid, mt)
+    t0 = time.perf_counter()
+    r, _, sm = lib.sign(p, sk, msg)
+    return r, sm, time.perf_counter() - t0
+
+
+def cpu_sign_baseline(oid: int, mt: bool, sks, msgs, want):
+    """Reference CPU signs/s on all host cores: the first `cores` signatures
+    of a mix set, one per spawned process (xmssmt_core_sign,
+    cuxmss/xmss_core.c:183-273, which builds every layer's subtree for each
+    signature), each compared with this library's signature."""
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    jobs = [(oid, mt, bytes(sks[i]), msgs[i]) for i in range(min(cores, len(msgs)))]
+    bound = os.sched_getaffinity(0)
+    os.sched_setaffinity(0, range(cores))  # the workers use every host core
+    try:
+        with mp.get_context("spawn").Pool(len(jobs)) as pool:
+            pool.map(abs, range(len(jobs)))  # workers started before the clock
+            t0 = time.perf_counter()
+            res = pool.map(_cpu_sign_one, jobs, chunksize=1)
+            dt = time.perf_counter() - t0
+    finally:
+        os.sched_setaffinity(0, bound)
+    correct = all(r == 0 and sm == want[i] for i, (r, sm, _) in enumerate(res))
+    return {"value": len(jobs) / dt, "unit": "signs/s", "cores": cores,
+            "kind": "reference" if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libxmssref.so")) else "port",
+            "sample": f"the set's first {len(jobs)} signatures, one per process, in {dt:.2f} s "
+                      f"(per signature {min(r[2] for r in res):.2f}-{max(r[2] for r in res):.2f} s)",
+            "correct": correct}
+
+
 def cpu_keygen_baseline(xb):
     """Reference CPU keygen leaves/s on all host cores: one XMSS-SHA2_10_256
     keypair per core (xmssmt_core_seed_keypair, cuxmss/xmss_core.c:134-161),
@@ -909,7 +951,7 @@ def run_mix(args):
     return mix_rates(xb, torch, dev, sh)
 
 
-def mix_rates(xb, torch, dev, sh):
+def mix_rates(xb, torch, dev, sh, cpu: bool = False):
     """Signs/s and verifies/s of the four mix sets, each set's chain kernels
     against the compression rate of its own hash core, and a byte check of
     every signature against the golden digests (tests/golden/mix_config4.json,
@@ -947,6 +989,7 @@ def mix_rates(xb, torch, dev, sh):
         smbuf, smoff, _ = xb.pack([b"\0" * (p.sig_bytes + len(m)) for m in msgs], align=16)
         smlen = np.zeros(count, np.uint64)
         ret = np.zeros(count, np.int32)
+        rows_before = rows.copy()  # the call advances the keys in place
         t0 = time.perf_counter()
         xb.sign_batch_packed(mt, rows, mbuf, moff, mln, smbuf, smoff, smlen, ret)
         t_sign = time.perf_counter() - t0
@@ -977,6 +1020,10 @@ def mix_rates(xb, torch, dev, sh):
         g = gold.get(name)
         byte_exact = None if g is None else (digest == g["sms_sha256"] and
                                              [pk[4:].tobytes().hex() for pk in pks] == g["pks"])
+        if cpu and not out["sets"]:
+            # the reference signs the set's first signatures on the host cores
+            # (XMSS^MT 20/2: two subtrees of 1,024 leaves built per signature)
+            cpu_sign = cpu_sign_baseline(oid, mt, [r[4:] for r in rows_before], msgs, sms)
         out["sets"].append({"set": name, "keys": nkeys, "signs": count, "first_index": start,
                             "signs_per_s": count / t_sign, "chain_roofline": roof,
                             "verifies_per_s": count / t_ver, "sign_s": t_sign, "verify_s": t_ver,
@@ -986,6 +1033,9 @@ def mix_rates(xb, torch, dev, sh):
                                             "h_calls": w.h_calls}})
         log(out["sets"][-1])
     out["correct"] = all(s["all_signed"] and s["all_verified"] and s["byte_exact_vs_oracle"] for s in out["sets"])
+    if cpu:
+        out["sets"][0]["cpu_baseline"] = cpu_sign
+        out["correct"] = out["correct"] and cpu_sign["correct"]
     return out
 
 
