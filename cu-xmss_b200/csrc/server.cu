@@ -7,7 +7,8 @@
 // the host and launches it on the slot's stream, then goes back to the queue
 // while that batch runs, so several batches overlap on the device.  Planning
 // and launching, and reaping finished slots, hold launch_mu, which add_key
-// also takes before it touches the key tables.
+// also takes before it touches the key tables.  A monitor thread reads the
+// device's free memory for admission every 20 ms.
 //
 // Signing with resident keys.  The reference recomputes the whole subtree
 // for every signature (treehash, xmss_core.c:253-270).  Here each subtree a
@@ -333,6 +334,14 @@ struct xmss_b200_server {
     std::vector<std::unique_ptr<Slot>> slots;
     std::unique_ptr<CopyPool> copies;
     std::thread thread;
+    // Free device memory for admission, read by the monitor thread: on B200
+    // a cudaMemGetInfo call took 4-90 ms at times while batches were in
+    // flight, which on the dispatcher thread stalled every request behind it.
+    std::atomic<uint64_t> free_bytes{0};
+    std::atomic<uint64_t> admitted_since{0};  // growth admitted since the last reading
+    std::thread monitor;
+    std::condition_variable monitor_cv;  // wakes the monitor at stop
+    void watch_memory();
 
     void run();
     Launch launch(Slot& s, std::vector<std::unique_ptr<Request>>& reqs,
@@ -466,13 +475,25 @@ Launch xmss_b200_server::launch(Slot& s, std::vector<std::unique_ptr<Request>>& 
         est += std::min<size_t>(tree_scratch, 3ull << 30);
     }
     if (est > s.admitted) {
-        size_t freeb = 0, totalb = 0;
-        XB_CUDA(cudaMemGetInfo(&freeb, &totalb));
-        if (freeb < est - s.admitted + cfg.mem_reserve_bytes) {
+        // against the monitor's last reading less the growth admitted since;
+        // only when that says no is the device asked again, here
+        const uint64_t need = est - s.admitted + cfg.mem_reserve_bytes;
+        const uint64_t since = admitted_since.load();
+        uint64_t freeb = free_bytes.load();
+        freeb = freeb > since ? freeb - since : 0;
+        if (freeb < need) {
+            size_t f = 0, totalb = 0;
+            XB_CUDA(cudaMemGetInfo(&f, &totalb));
+            free_bytes = f;
+            admitted_since = 0;
+            freeb = f;
+        }
+        if (freeb < need) {
             std::lock_guard<std::mutex> g(mu);
             stats.deferred_for_memory++;
             return Launch::kDeferred;
         }
+        admitted_since += est - s.admitted;
     }
     batch_seq++;
 
@@ -709,7 +730,7 @@ Launch xmss_b200_server::launch(Slot& s, std::vector<std::unique_ptr<Request>>& 
     }
     std::sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
     const size_t nl = std::min(order.size(), kMaxLanes);
-    while (s.lanes.size() < nl) {
+    while (s.lanes.size() < nl) {  // lanes are made at create; a fallback only
         auto ln = std::make_unique<Lane>();
         XB_CUDA(cudaStreamCreateWithFlags(&ln->st, cudaStreamNonBlocking));
         XB_CUDA(cudaEventCreate(&ln->start));
@@ -861,6 +882,24 @@ void xmss_b200_server::finish(Slot& s)
     for (auto& rp : s.reqs) complete_locked(*rp);
     s.reqs.clear();
     done_cv.notify_all();
+}
+
+// Reads the device's free memory every 20 ms until the server stops.
+void xmss_b200_server::watch_memory()
+{
+    cudaSetDevice(device);
+    std::unique_lock<std::mutex> lk(mu);
+    while (!stop) {
+        lk.unlock();
+        size_t f = 0, t = 0;
+        const uint64_t since = admitted_since.load();
+        if (cudaMemGetInfo(&f, &t) == cudaSuccess) {
+            free_bytes = f;
+            admitted_since -= std::min<uint64_t>(since, admitted_since.load());
+        }
+        lk.lock();
+        monitor_cv.wait_for(lk, std::chrono::milliseconds(20), [this] { return stop; });
+    }
 }
 
 void xmss_b200_server::run()
@@ -1055,13 +1094,29 @@ extern "C" int xmss_b200_server_create(const xmss_b200_server_config* cfg, xmss_
             s->stage.keep_old_blocks();
             s->stage.get(stage);
             s->dev.get(stage);
+            // every lane up front: creating streams and events while batches
+            // run took 8-34 ms of the dispatcher's time on B200
+            while (s->lanes.size() < kMaxLanes) {
+                auto ln = std::make_unique<Lane>();
+                XB_CUDA(cudaStreamCreateWithFlags(&ln->st, cudaStreamNonBlocking));
+                XB_CUDA(cudaEventCreate(&ln->start));
+                XB_CUDA(cudaEventCreate(&ln->done));
+                ln->w.order_on(ln->st);
+                s->lanes.push_back(std::move(ln));
+            }
             srv->slots.push_back(std::move(s));
         }
         for (auto& sp : srv->slots) XB_CUDA(cudaStreamSynchronize(sp->st));
         srv->copies = std::make_unique<CopyPool>(
             std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 4)));
+        {
+            size_t f = 0, t = 0;
+            XB_CUDA(cudaMemGetInfo(&f, &t));
+            srv->free_bytes = f;
+        }
         xmss_b200_server* p = srv.release();
         p->thread = std::thread([p] { p->run(); });
+        p->monitor = std::thread([p] { p->watch_memory(); });
         *out = p;
         return 0;
     } catch (const std::exception& ex) {
@@ -1077,7 +1132,9 @@ extern "C" void xmss_b200_server_destroy(xmss_b200_server* srv)
         srv->stop = true;
     }
     srv->cv.notify_all();
+    srv->monitor_cv.notify_all();
     if (srv->thread.joinable()) srv->thread.join();
+    if (srv->monitor.joinable()) srv->monitor.join();
     cudaSetDevice(srv->device);
     for (auto& s : srv->slots) {
         for (auto& ln : s->lanes) {
