@@ -352,8 +352,10 @@ int xmss_b200_sign_open_device_noalloc(uint32_t oid, int mt, uint32_t count, con
  * dispatcher thread batches whatever is queued whenever one of `slots` batch
  * slots is free (continuous batching: batches admitted while others run
  * overlap on the device), groups each batch by operation and parameter set,
- * and admits it only while free device memory (cudaMemGetInfo) stays above
- * mem_reserve_bytes, shrinking the batch when it does not fit.
+ * and admits it only while free device memory stays above
+ * mem_reserve_bytes, shrinking the batch when it does not fit (free memory
+ * is read by a monitor thread every 20 ms, and asked again by the
+ * dispatcher only when that reading says a batch does not fit).
  *
  * Keys are resident on the device: seeds, PRF key, root, PUB_SEED, a u64
  * one-time index counter advanced with atomicAdd (reservations run in
