@@ -42,6 +42,35 @@ def test_serve_config1_byte_exact(xb, golden):
         assert st["completed"] == 34 and st["trees_built"] == 1
 
 
+def test_serve_admission_refuses_what_never_fits(xb, golden):
+    """Admission by free device memory: with a reserve larger than any GPU's
+    memory no batch fits, so the dispatcher halves each batch down to single
+    requests and refuses those with -3 (the deferrals are counted), before
+    any one-time index is taken: the key exports unchanged.  The free-memory
+    figure comes from the monitor thread; the dispatcher's own query, made
+    only when that figure says no, refuses too."""
+    g = golden("config1.json")
+    p = xb.parse_oid(1)
+    sk = bytes.fromhex(g["sk"])
+    with xb.Server(mem_reserve_bytes=1 << 60) as srv:
+        kid = srv.add_key(sk)
+        pk = bytes.fromhex(g["pk"])
+        sms = [bytes.fromhex(s) for s in g["sms"][:4]]
+        tags = [srv.submit_verify(s, pk) for s in sms] + [srv.submit_sign(kid, bytes.fromhex(m), p.sig_bytes)
+                                                          for m in g["msgs"][:3]]
+        res = srv.wait(tags)
+        assert [res[t]["ret"] for t in tags] == [-3] * len(tags)
+        assert srv.stats()["deferred_for_memory"] >= len(tags)
+        assert srv.export_sk(kid) == sk
+    with xb.Server() as srv:  # the same requests with the default reserve
+        kid = srv.add_key(sk)
+        tags = [srv.submit_verify(s, pk) for s in sms] + [srv.submit_sign(kid, bytes.fromhex(m), p.sig_bytes)
+                                                          for m in g["msgs"][:3]]
+        res = srv.wait(tags)
+        assert [res[t]["ret"] for t in tags] == [0] * len(tags)
+        assert [res[t]["sm"].hex() for t in tags[4:]] == g["sms"][:3]
+
+
 def test_serve_every_family_mt(xb, golden):
     """The reference's XMSS^MT 20/4 signatures of all seven hash families at
     seeded indices, signed by the server from keys resumed at those indices
