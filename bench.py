@@ -18,7 +18,7 @@ value      verifies/s with inputs resident in HBM, CUDA events around each
            (all three are reported in config)
 e2e        the same through the host-buffer C-ABI from pinned host memory,
            every step's copies included: xmss_b200_sign_open_batch_async on
-           four streams in turn (steps' copies overlap other steps'
+           eight streams in turn (steps' copies overlap other steps'
            kernels) over 16 distinct pinned copies of the input taken in
            turn (221 MB > L2, in place of a flush), wall clock over all
            steps; the blocking
@@ -57,7 +57,7 @@ sys.path.insert(0, os.path.join(ROOT, "cu-xmss_b200"))
 
 NUM_SIGS = 4096
 NUM_KEYS = 64
-E2E_STREAMS = 4  # streams the e2e leg takes in turn
+E2E_STREAMS = 8  # streams the e2e leg takes in turn
 E2E_INPUTS = 16  # distinct host copies of its input (16 x 13.8 MB > 126 MB L2)
 OID = 0x01  # XMSS-SHA2_10_256
 SEED = 20260303
