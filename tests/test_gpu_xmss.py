@@ -426,6 +426,56 @@ def test_verify_graph_replays(xb, count):
     g.close()
 
 
+def test_verify_graphs_concurrent_on_streams(xb):
+    """Verify graphs own their scratch, so several of them, each over its
+    own batch, replay concurrently on several streams (the pipelined form of
+    the benchmark): every replay's statuses equal the blocking call's for its
+    batch, including split (1,100-signature) and unsplit batches in flight
+    together, each graph replayed twice with nothing in between."""
+    import torch
+
+    rng = np.random.default_rng(97)
+    keys = 3
+    seeds = np.frombuffer(rng.bytes(keys * 96), np.uint8).reshape(keys, 96)
+    pks, sks = xb.keypair_batch(1, False, seeds)
+    dev = torch.device("cuda", 0)
+    d_pk = torch.from_numpy(np.ascontiguousarray(pks[:, 4:])).to(dev)
+    items = []
+    for count in (1100, 300, 1100, 64):
+        keyix = rng.integers(0, keys, count).astype(np.uint32)
+        rows = np.array(sks[keyix])
+        idx = rng.integers(0, 1023, count)
+        for i in range(count):
+            rows[i, 4:8] = np.frombuffer(int(idx[i]).to_bytes(4, "big"), np.uint8)
+        msgs = [rng.bytes(int(L)) for L in np.exp(rng.uniform(0, np.log(4000), count)).astype(int)]
+        _, sms = xb.sign_batch(False, rows, msgs)
+        sms = [bytearray(s) for s in sms]
+        for i in range(int(rng.integers(0, 4)), count, 4):
+            sms[i][int(rng.integers(0, len(sms[i])))] ^= 1
+        buf, off, ln = xb.pack([bytes(s) for s in sms], align=16)
+        want = xb.sign_open_batch(False, buf, off, ln, pks, keyix)
+        d = dict(sm=torch.from_numpy(buf).to(dev), off=torch.from_numpy(off.astype(np.int64)).to(dev),
+                 ln=torch.from_numpy(ln.astype(np.int64)).to(dev), kix=torch.from_numpy(keyix.astype(np.int32)).to(dev),
+                 st=torch.full((count,), 7, dtype=torch.int32, device=dev), want=want, count=count)
+        d["g"] = xb.VerifyGraph(1, False, count, d["sm"].data_ptr(), d["off"].data_ptr(), d["ln"].data_ptr(),
+                                d_pk.data_ptr(), keys, d["kix"].data_ptr(), d["st"].data_ptr())
+        items.append(d)
+    streams = [torch.cuda.Stream() for _ in range(len(items))]
+    torch.cuda.synchronize()
+    for rep in range(2):
+        for d in items:
+            d["st"].fill_(7)
+        torch.cuda.synchronize()
+        for d, s in zip(items, streams):
+            d["g"].launch(s.cuda_stream)
+            d["g"].launch(s.cuda_stream)
+        torch.cuda.synchronize()
+        for k, d in enumerate(items):
+            assert (d["st"].cpu().numpy() == d["want"]).all(), (rep, k)
+    for d in items:
+        d["g"].close()
+
+
 def test_results_do_not_depend_on_launch_shape(xb, golden):
     """Every tunable shape (CTA sizes 32 / 64 / 128, split on or off at any
     H_msg boundary) gives the same accept bitmap and the same keys; the
